@@ -1,0 +1,73 @@
+/* CPU oracle for the direct J/K Fock build — TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain C++ restatement of Dalton's HERMIT two-electron Fock path, used by
+ * tests/, __graft_entry__.smoke() and the CPU-baseline legs of bench.py as the
+ * checker.  Nothing in the product (dalton_b200/, include/) links or calls it.
+ *
+ * Parity is pinned by Dalton's stored golden outputs: the H2O/cc-pVDZ direct
+ * RHF energy (DALTON/test/trueresult/energy_direct.ref:659) and the acrolein
+ * HF/STO-3G energy and molecular gradient
+ * (DALTON/test/geoopt_preopt2/result/preopt_acrolein.out:637,840-850).
+ *
+ * The basis arrives in Dalton block form (one block = one atom's shell of
+ * angular momentum l with nprim primitives and ncontr contracted functions,
+ * CPRIM coefficients already NRMORB-normalised), AOs in Dalton C1 order.
+ */
+#ifndef DGF_ORACLE_H
+#define DGF_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int64_t nblock, natom, nbf, spherical;
+  const int64_t *block_l, *block_atom, *block_nprim, *block_ncontr;
+  const int64_t *block_ao_offset, *block_prim_offset, *block_coef_offset;
+  const double *prim_exp, *coef; /* coef: per block column-major (nprim, ncontr) */
+  const double *atom_xyz;        /* (natom, 3) bohr */
+  const double *atom_charge;     /* (natom,) */
+} orc_basis;
+
+/* Number of OpenMP threads the oracle uses (0 = all). */
+void orc_set_threads(int n);
+int orc_get_threads(void);
+
+/* Boys function F_0..F_m(T) (own series / asymptotic evaluation). */
+void orc_boys(int m, double t, double *f);
+
+/* Cartesian -> spherical matrix, (2l+1) x ncart(l) row-major (SPHCO1, MINTEG=2). */
+void orc_sph_matrix(int l, double *out);
+
+/* One-electron S, T, V (N x N, row-major; symmetric). */
+int orc_oneint(const orc_basis *b, double *S, double *T, double *V);
+
+/* Full ERI tensor (N^4, (pq|rs) at ((p*N+q)*N+r)*N+s) for small checks. */
+int orc_eri_full(const orc_basis *b, double *eri);
+
+/* Schwarz factors per segmented shell pair: Q_AB = sqrt(max |(ab|ab)|).
+ * Returns the number of segmented shells in *nshell. */
+int orc_nshell(const orc_basis *b);
+
+/* Fock build with HERFCK semantics (FMAT overwritten):
+ *   IFCTYP = 10*X + Y; X = 1 symmetric D, 0 general, 2 antisymmetric;
+ *   Y = 1 Coulomb, 2 exchange, 3 both.
+ *   F = [Y&1] J[D] - [Y&2] (hfxfac/2) K[D],
+ *   J_pq = sum_rs (pq|rs) (D_rs + D_sr)/2, K_pq = sum_rs (pr|qs) D_rs.
+ * Shell quartets with Q_AB * Q_CD < thrs are skipped (segmented shells).
+ * Matrices are N x N row-major; ndmat densities back to back. */
+int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat,
+             double *fmat, double hfxfac, double thrs);
+
+/* Two-electron part of the RHF gradient: 1/2 sum (pq|rs)^x [D_pq D_rs - hfx/2 D_pr D_qs],
+ * D the total (symmetric) density; grad (natom, 3) overwritten. */
+int orc_grad2e(const orc_basis *b, const double *dmat, double hfxfac, double thrs, double *grad);
+
+/* One-electron + nuclear-repulsion part of the RHF gradient:
+ *   sum D_pq h_pq^x - sum W_pq S_pq^x + dVnn/dx; grad (natom, 3) overwritten. */
+int orc_grad1e(const orc_basis *b, const double *dmat, const double *wmat, double *grad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
