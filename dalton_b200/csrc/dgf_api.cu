@@ -1,0 +1,766 @@
+// Host runtime and C ABI of libdgfock: context (device-resident shell-pair
+// data, Schwarz factors, class-sorted pair lists), the HERFCK-semantics Fock
+// build, and the Boys/spherical tables.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "dgf_internal.h"
+#include "dgf_md.cuh"
+
+using namespace dgf;
+
+// ------------------------------------------------------------------ errors
+namespace dgf {
+static thread_local std::string g_last_error;
+void set_error(const char *file, int line, const std::string &msg) {
+  const char *f = strrchr(file, '/');
+  g_last_error = std::string(f ? f + 1 : file) + ":" + std::to_string(line) + ": " + msg;
+}
+}  // namespace dgf
+
+#define DGF_FAIL(code, msg)                \
+  do {                                     \
+    ::dgf::set_error(__FILE__, __LINE__, msg); \
+    return code;                           \
+  } while (0)
+
+// Test hook: DGF_FAULT_INJECT=alloc makes every device allocation of the
+// library fail, so callers' error paths can be exercised without a GPU fault.
+static bool alloc_fault_injected() {
+  const char *e = getenv("DGF_FAULT_INJECT");
+  return e && strcmp(e, "alloc") == 0;
+}
+
+template <typename T>
+static cudaError_t dev_alloc(T **p, size_t n) {
+  if (alloc_fault_injected()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+}
+
+// ------------------------------------------------------------------ tables
+namespace dgf {
+
+// F_m(t) by its power series, e^-t sum_k (2t)^k / ((2m+1)(2m+3)...(2m+2k+1)),
+// in long double (all terms positive; accurate to ~1e-18 relative for t < 60).
+static long double boys_series(int m, long double t) {
+  long double term = 1.0L / (2 * m + 1), sum = term;
+  for (int k = 1; k < 4000; ++k) {
+    term *= 2.0L * t / (2 * m + 2 * k + 1);
+    sum += term;
+    if (term < 1e-22L * sum) break;
+  }
+  return expl(-t) * sum;
+}
+
+double boys_reference(int m, double t) {
+  if (t < 60.0) return (double)boys_series(m, t);
+  long double f = 0.5L * sqrtl(3.14159265358979323846264338327950288L / t);
+  long double et = expl(-(long double)t);
+  for (int j = 0; j < m; ++j) f = ((2 * j + 1) * f - et) / (2.0L * t);
+  return (double)f;
+}
+
+// Chebyshev interpolant of F_M on each interval at kBoysNcoef nodes, written
+// out as a polynomial in the interval's local variable x in [-1, 1].
+void boys_table_host(std::vector<double> &out) {
+  const int n = kBoysNcoef;
+  const long double pi = 3.14159265358979323846264338327950288L;
+  out.assign((size_t)(kBoysMaxM + 1) * kBoysTableDoubles, 0.0);
+  std::vector<long double> f(n), c(n), tk(n * n), pw(n);
+  // monomial coefficients of T_j(x): tk[j*n + k]
+  std::fill(tk.begin(), tk.end(), 0.0L);
+  tk[0] = 1.0L;
+  if (n > 1) tk[1 * n + 1] = 1.0L;
+  for (int j = 2; j < n; ++j)
+    for (int k = 0; k < n; ++k) {
+      long double v = -tk[(j - 2) * n + k];
+      if (k > 0) v += 2.0L * tk[(j - 1) * n + k - 1];
+      tk[j * n + k] = v;
+    }
+  const long double h = 1.0L / kBoysPerUnit;
+  for (int M = 0; M <= kBoysMaxM; ++M)
+    for (int i = 0; i < kBoysNint; ++i) {
+      const long double mid = (i + 0.5L) * h;
+      for (int k = 0; k < n; ++k) {
+        long double x = cosl(pi * (k + 0.5L) / n);
+        f[k] = boys_series(M, mid + 0.5L * h * x);
+      }
+      for (int j = 0; j < n; ++j) {
+        long double s = 0;
+        for (int k = 0; k < n; ++k) s += f[k] * cosl(pi * j * (k + 0.5L) / n);
+        c[j] = s * 2.0L / n;
+      }
+      c[0] *= 0.5L;
+      std::fill(pw.begin(), pw.end(), 0.0L);
+      for (int j = 0; j < n; ++j)
+        for (int k = 0; k < n; ++k) pw[k] += c[j] * tk[j * n + k];
+      for (int k = 0; k < n; ++k) out[(size_t)M * kBoysTableDoubles + i * n + k] = (double)pw[k];
+    }
+}
+
+// Cartesian -> real spherical coefficients with Dalton's conventions (SPHCO1,
+// DALTON/abacus/her1pro.F:4697-4770, MORDER=1 so m = -l..l, MINTEG=2 so the
+// functions are normalised given Cartesians carrying the x^l norm); p and s
+// are identities.  Layout per l: rows m, columns Cartesian components.
+void sph_table_host(std::vector<double> &out) {
+  out.assign(kSphTableDoubles, 0.0);
+  auto binom = [](int nn, int k) {
+    if (k < 0 || k > nn) return 0.0;
+    double r = 1.0;
+    for (int i = 1; i <= k; ++i) r = r * (nn - k + i) / i;
+    return r;
+  };
+  auto fact = [](int nn) {
+    double r = 1.0;
+    for (int i = 2; i <= nn; ++i) r *= i;
+    return r;
+  };
+  for (int l = 0; l <= kMaxShellL + 1; ++l) {
+    const int nx = ncart(l), nlm = 2 * l + 1;
+    double *T = out.data() + sph_offset(l);
+    if (l <= 1) {
+      for (int i = 0; i < nx; ++i) T[i * nx + i] = 1.0;
+      continue;
+    }
+    std::vector<double> pl(l + 2, 0.0), cs((l + 1) * (l + 1), 0.0);
+    for (int k = 0; k <= l / 2; ++k)
+      pl[l - 2 * k] = ((k % 2) ? -1.0 : 1.0) * std::ldexp(1.0, -l) * binom(l, k) * binom(2 * (l - k), l);
+    cs[0] = 1.0;
+    for (int m = 1; m <= l; ++m) {
+      cs[m * (l + 1)] = 1.0;
+      for (int k = 1; k <= m; ++k) {
+        cs[m * (l + 1) + k] = cs[(m - 1) * (l + 1) + k - 1] * (((k - 1) % 2) ? -1.0 : 1.0);
+        if (m > k) cs[m * (l + 1) + k] += cs[(m - 1) * (l + 1) + k];
+      }
+    }
+    double df = 1.0;
+    for (int v = 2 * l - 1; v > 0; v -= 2) df *= v;
+    for (int m = 0; m <= l; ++m) {
+      double cm = (m == 0) ? 1.0 : std::sqrt(2.0 * fact(l - m) / fact(l + m));
+      cm /= std::sqrt(df);
+      for (int k = (l - m) % 2; k <= l - m; k += 2) {
+        if (m > 0) pl[k] = (k + 1) * pl[k + 1];
+        const double cmk = cm * pl[k];
+        for (int i = 0; i <= (l - k - m) / 2; ++i) {
+          const double cmki = cmk * binom((l - k - m) / 2, i);
+          for (int j = 0; j <= i; ++j) {
+            const double cmkij = cmki * binom(i, j);
+            for (int nn = 0; nn <= m; ++nn) {
+              int ix = l - 2 * j - m + nn;
+              ix = ix * (ix + 1) / 2 + l + 1 - m - 2 * i;  // 1-based Cartesian index
+              const int ilm = (nn % 2 == 1) ? (l - m) : (l + m);  // 0-based row
+              T[ilm * nx + (ix - 1)] += cmkij * cs[m * (l + 1) + nn];
+            }
+          }
+        }
+      }
+    }
+    (void)nlm;
+  }
+}
+
+}  // namespace dgf
+
+// ----------------------------------------------------------------- context
+struct ClassPlan {
+  int X, Y;
+  int64_t off;        // offset of this class pair's qoff array in the plan buffer
+  int64_t nquartet;
+};
+
+struct dgf_ctx {
+  int device = 0, nbf = 0, natom = 0, nshell = 0, spherical = 1, maxl = 0, nsm = 148;
+  std::vector<double> xyz, charge;
+  std::vector<int> sh_l, sh_atom, sh_ao, sh_nprim, sh_p0;
+  std::vector<double> sh_a, sh_c;
+  std::vector<PairRec> pairs;  // class-major, Schwarz-descending inside a class
+  int cls_off[kNumPairClass + 1] = {0};
+  std::vector<PrimPair> pp;
+  PairRec *d_pairs = nullptr;
+  PrimPair *d_pp = nullptr;
+  double *d_boys = nullptr, *d_sph = nullptr;
+  // per-call buffers
+  int cap_slots = 0, cap_io = 0;
+  double *d_D = nullptr, *d_Ds = nullptr, *d_Fh = nullptr, *d_io = nullptr;
+  float *d_dmax = nullptr;
+  unsigned long long *d_cnt = nullptr;
+  // quartet plan, cached by Schwarz threshold
+  double plan_thrs = -1.0;
+  std::vector<ClassPlan> plan;
+  int64_t *d_qoff = nullptr;
+  size_t qoff_cap = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static void free_ctx(dgf_ctx *c) {
+  if (!c) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(c->device);
+  void *ptrs[] = {c->d_pairs, c->d_pp, c->d_boys, c->d_sph, c->d_D, c->d_Ds, c->d_Fh,
+                  c->d_io, c->d_dmax, c->d_cnt, c->d_qoff};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  cudaSetDevice(prev);
+  delete c;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+static int launch_class(dgf_ctx *c, int X, int Y, JKArgs &args, cudaStream_t st) {
+  const ClassKernel &k = jk_kernel(X, Y, 0);
+  int64_t grid64 = std::min<int64_t>(args.nquartet, (int64_t)c->nsm * 16);
+  int grid = (int)std::max<int64_t>(grid64, 1);
+  k.launch(args, grid, k.block, k.smem, st);
+  DGF_CUDA_CHECK(cudaGetLastError());
+  return DGF_OK;
+}
+
+static JKArgs base_args(dgf_ctx *c) {
+  JKArgs a;
+  memset(&a, 0, sizeof(a));
+  a.pp = c->d_pp;
+  a.sph = c->d_sph;
+  a.spherical = c->spherical;
+  a.nbf = c->nbf;
+  a.nshell = c->nshell;
+  return a;
+}
+
+// Schwarz factors: (ab|ab) of every pair with the diag mode of the kernels
+// (GABGEN/GABDRV, DALTON/abacus/her2gab.F:36,1776).
+static int compute_schwarz(dgf_ctx *c) {
+  const int np = (int)c->pairs.size();
+  double *d_q = nullptr;
+  DGF_CUDA_CHECK(dev_alloc(&d_q, np));
+  for (int X = 0; X < kNumPairClass; ++X) {
+    const int n = c->cls_off[X + 1] - c->cls_off[X];
+    if (!n) continue;
+    const int la = (X == 0) ? 0 : (X <= 2) ? 1 : (X <= 5) ? 2 : 3;
+    JKArgs a = base_args(c);
+    a.bra = a.ket = c->d_pairs + c->cls_off[X];
+    a.nbra = n;
+    a.nquartet = n;
+    a.same_class = 1;
+    a.boys = c->d_boys + (size_t)(2 * (la + (X - la * (la + 1) / 2))) * kBoysTableDoubles;
+    a.diag_out = d_q + c->cls_off[X];
+    int st = launch_class(c, X, X, a, c->stream);
+    if (st) {
+      cudaFree(d_q);
+      return st;
+    }
+  }
+  std::vector<double> q(np);
+  cudaError_t e = cudaMemcpyAsync(q.data(), d_q, np * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d_q);
+  DGF_CUDA_CHECK(e);
+  for (int i = 0; i < np; ++i) c->pairs[i].Q = q[i];
+  return DGF_OK;
+}
+
+extern "C" void dgf_default_options(dgf_options *opt) {
+  if (!opt) return;
+  opt->thrs = 1e-12;
+  opt->ifthrs = 20;
+  opt->hfxfac = 1.0;
+  opt->mixed_cutoff = 0.0;
+}
+
+extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
+  if (!out) DGF_FAIL(DGF_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!b || b->nblock <= 0 || b->natom <= 0 || b->nbf <= 0) DGF_FAIL(DGF_ERR_ARG, "empty or invalid basis");
+  if (!b->block_l || !b->block_atom || !b->block_nprim || !b->block_ncontr || !b->block_ao_offset ||
+      !b->block_prim_offset || !b->block_coef_offset || !b->prim_exp || !b->coef || !b->atom_xyz ||
+      !b->atom_charge)
+    DGF_FAIL(DGF_ERR_ARG, "basis has a NULL array");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    DGF_FAIL(DGF_ERR_NODEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= ndev) DGF_FAIL(DGF_ERR_ARG, "device index out of range");
+  std::unique_ptr<dgf_ctx, void (*)(dgf_ctx *)> c(new dgf_ctx, free_ctx);
+  c->device = device;
+  DeviceGuard g(device);
+  cudaDeviceProp prop;
+  DGF_CUDA_CHECK(cudaGetDeviceProperties(&prop, device));
+  c->nsm = prop.multiProcessorCount;
+  c->nbf = (int)b->nbf;
+  c->natom = (int)b->natom;
+  c->spherical = b->spherical ? 1 : 0;
+  c->xyz.assign(b->atom_xyz, b->atom_xyz + 3 * b->natom);
+  c->charge.assign(b->atom_charge, b->atom_charge + b->natom);
+
+  // Segment Dalton's general-contraction blocks into one shell per
+  // contracted function (zero coefficients dropped).
+  for (dgf_int ib = 0; ib < b->nblock; ++ib) {
+    const int l = (int)b->block_l[ib];
+    if (l < 0 || l > kMaxShellL) DGF_FAIL(DGF_ERR_UNSUPPORTED, "angular momentum above f is not supported");
+    const int np = (int)b->block_nprim[ib], nc = (int)b->block_ncontr[ib];
+    const int at = (int)b->block_atom[ib];
+    if (np <= 0 || nc <= 0 || at < 0 || at >= c->natom) DGF_FAIL(DGF_ERR_ARG, "invalid block");
+    const int nf = nfun(l, c->spherical);
+    for (int k = 0; k < nc; ++k) {
+      const int ao = (int)b->block_ao_offset[ib] + k * nf;
+      if (ao < 0 || ao + nf > c->nbf) DGF_FAIL(DGF_ERR_ARG, "AO offset out of range");
+      c->sh_l.push_back(l);
+      c->sh_atom.push_back(at);
+      c->sh_ao.push_back(ao);
+      c->sh_p0.push_back((int)c->sh_a.size());
+      int cnt = 0;
+      for (int i = 0; i < np; ++i) {
+        const double cc = b->coef[b->block_coef_offset[ib] + (dgf_int)k * np + i];
+        const double ex = b->prim_exp[b->block_prim_offset[ib] + i];
+        if (cc == 0.0) continue;
+        if (!(ex > 0.0)) DGF_FAIL(DGF_ERR_ARG, "non-positive exponent");
+        c->sh_a.push_back(ex);
+        c->sh_c.push_back(cc);
+        ++cnt;
+      }
+      c->sh_nprim.push_back(cnt);
+      c->maxl = std::max(c->maxl, l);
+    }
+  }
+  c->nshell = (int)c->sh_l.size();
+
+  // Shell pairs A >= B (the higher l first) with their primitive pairs;
+  // primitive pairs with mu |AB|^2 > 40 (e^-40 ~ 4e-18) are dropped.
+  const double r2pi52 = std::sqrt(2.0 * std::pow(3.14159265358979323846, 2.5));
+  std::vector<std::vector<PairRec>> bycls(kNumPairClass);
+  std::vector<PrimPair> pp;
+  for (int A = 0; A < c->nshell; ++A)
+    for (int B = 0; B <= A; ++B) {
+      int sa = A, sb = B;
+      if (c->sh_l[sb] > c->sh_l[sa]) std::swap(sa, sb);
+      const int la = c->sh_l[sa], lb = c->sh_l[sb];
+      const double *xa = &c->xyz[3 * c->sh_atom[sa]], *xb = &c->xyz[3 * c->sh_atom[sb]];
+      const double ab2 = (xa[0] - xb[0]) * (xa[0] - xb[0]) + (xa[1] - xb[1]) * (xa[1] - xb[1]) +
+                         (xa[2] - xb[2]) * (xa[2] - xb[2]);
+      PairRec r;
+      memset(&r, 0, sizeof(r));
+      r.shA = sa;
+      r.shB = sb;
+      r.aoA = c->sh_ao[sa];
+      r.aoB = c->sh_ao[sb];
+      r.same = (A == B);
+      r.atA = c->sh_atom[sa];
+      r.atB = c->sh_atom[sb];
+      r.pp0 = (int)pp.size();
+      for (int i = 0; i < c->sh_nprim[sa]; ++i)
+        for (int j = 0; j < c->sh_nprim[sb]; ++j) {
+          const double ea = c->sh_a[c->sh_p0[sa] + i], eb = c->sh_a[c->sh_p0[sb] + j];
+          const double p = ea + eb, mu = ea * eb / p;
+          if (mu * ab2 > 40.0) continue;
+          PrimPair q;
+          q.p = p;
+          q.Px = (ea * xa[0] + eb * xb[0]) / p;
+          q.Py = (ea * xa[1] + eb * xb[1]) / p;
+          q.Pz = (ea * xa[2] + eb * xb[2]) / p;
+          q.PAx = q.Px - xa[0];
+          q.PAy = q.Py - xa[1];
+          q.PAz = q.Pz - xa[2];
+          q.PBx = q.Px - xb[0];
+          q.PBy = q.Py - xb[1];
+          q.PBz = q.Pz - xb[2];
+          q.K = c->sh_c[c->sh_p0[sa] + i] * c->sh_c[c->sh_p0[sb] + j] * std::exp(-mu * ab2) * r2pi52 / p;
+          q.pad = 0.0;
+          pp.push_back(q);
+        }
+      r.npp = (int)pp.size() - r.pp0;
+      if (r.npp == 0) continue;
+      bycls[pair_class(la, lb)].push_back(r);
+    }
+  c->pp.swap(pp);
+  c->cls_off[0] = 0;
+  for (int X = 0; X < kNumPairClass; ++X) {
+    c->cls_off[X + 1] = c->cls_off[X] + (int)bycls[X].size();
+    c->pairs.insert(c->pairs.end(), bycls[X].begin(), bycls[X].end());
+  }
+
+  DGF_CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  DGF_CUDA_CHECK(cudaEventCreate(&c->ev0));
+  DGF_CUDA_CHECK(cudaEventCreate(&c->ev1));
+  DGF_CUDA_CHECK(jk_prepare_all());
+  std::vector<double> boys, sph;
+  boys_table_host(boys);
+  sph_table_host(sph);
+  if (dev_alloc(&c->d_boys, boys.size()) != cudaSuccess || dev_alloc(&c->d_sph, sph.size()) != cudaSuccess ||
+      dev_alloc(&c->d_pp, c->pp.size()) != cudaSuccess || dev_alloc(&c->d_pairs, c->pairs.size()) != cudaSuccess ||
+      dev_alloc(&c->d_cnt, 8) != cudaSuccess) {
+    cudaGetLastError();
+    DGF_FAIL(DGF_ERR_NOMEM, "device allocation failed while creating the context");
+  }
+  DGF_CUDA_CHECK(cudaMemcpy(c->d_boys, boys.data(), boys.size() * 8, cudaMemcpyHostToDevice));
+  DGF_CUDA_CHECK(cudaMemcpy(c->d_sph, sph.data(), sph.size() * 8, cudaMemcpyHostToDevice));
+  DGF_CUDA_CHECK(cudaMemcpy(c->d_pp, c->pp.data(), c->pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice));
+  DGF_CUDA_CHECK(
+      cudaMemcpy(c->d_pairs, c->pairs.data(), c->pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice));
+  int st = compute_schwarz(c.get());
+  if (st) return st;
+  // Sort each class by Schwarz factor, descending, and re-upload.
+  for (int X = 0; X < kNumPairClass; ++X)
+    std::stable_sort(c->pairs.begin() + c->cls_off[X], c->pairs.begin() + c->cls_off[X + 1],
+                     [](const PairRec &u, const PairRec &v) { return u.Q > v.Q; });
+  DGF_CUDA_CHECK(
+      cudaMemcpy(c->d_pairs, c->pairs.data(), c->pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice));
+  *out = c.release();
+  return DGF_OK;
+}
+
+extern "C" void dgf_destroy(dgf_ctx *c) { free_ctx(c); }
+
+extern "C" int dgf_info(const dgf_ctx *c, dgf_int *nbf, dgf_int *natom, dgf_int *nshell) {
+  if (!c) DGF_FAIL(DGF_ERR_ARG, "ctx is NULL");
+  if (nbf) *nbf = c->nbf;
+  if (natom) *natom = c->natom;
+  if (nshell) *nshell = c->nshell;
+  return DGF_OK;
+}
+
+// Quartet plan: for every class pair X >= Y and bra pair, the number of ket
+// pairs with Q_AB Q_CD >= thrs (a prefix of the Schwarz-sorted ket list, and
+// only kets up to the bra itself when X == Y), as prefix sums.
+static int build_plan(dgf_ctx *c, double thrs) {
+  if (c->plan_thrs == thrs && !c->plan.empty()) return DGF_OK;
+  std::vector<int64_t> all;
+  std::vector<ClassPlan> plan;
+  for (int X = 0; X < kNumPairClass; ++X)
+    for (int Y = 0; Y <= X; ++Y) {
+      const int nb = c->cls_off[X + 1] - c->cls_off[X], nk = c->cls_off[Y + 1] - c->cls_off[Y];
+      if (!nb || !nk) continue;
+      const PairRec *bra = &c->pairs[c->cls_off[X]], *ket = &c->pairs[c->cls_off[Y]];
+      ClassPlan cp;
+      cp.X = X;
+      cp.Y = Y;
+      cp.off = (int64_t)all.size();
+      int64_t acc = 0;
+      all.push_back(0);
+      for (int i = 0; i < nb; ++i) {
+        const double qb = bra[i].Q;
+        int lo = 0, hi = nk;  // first ket with qb*Q < thrs
+        while (lo < hi) {
+          int mid = (lo + hi) >> 1;
+          if (qb * ket[mid].Q >= thrs)
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        int n = lo;
+        if (X == Y) n = std::min(n, i + 1);
+        acc += n;
+        all.push_back(acc);
+      }
+      cp.nquartet = acc;
+      if (acc > 0) plan.push_back(cp);
+    }
+  if (all.size() > c->qoff_cap) {
+    if (c->d_qoff) cudaFree(c->d_qoff);
+    c->d_qoff = nullptr;
+    if (dev_alloc(&c->d_qoff, all.size()) != cudaSuccess) {
+      cudaGetLastError();
+      c->qoff_cap = 0;
+      DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the quartet plan failed");
+    }
+    c->qoff_cap = all.size();
+  }
+  DGF_CUDA_CHECK(cudaMemcpy(c->d_qoff, all.data(), all.size() * 8, cudaMemcpyHostToDevice));
+  c->plan.swap(plan);
+  c->plan_thrs = thrs;
+  return DGF_OK;
+}
+
+static int ensure_slots(dgf_ctx *c, int nslot) {
+  if (nslot <= c->cap_slots) return DGF_OK;
+  const size_t n2 = (size_t)c->nbf * c->nbf;
+  for (double **p : {&c->d_D, &c->d_Ds, &c->d_Fh}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  c->cap_slots = 0;
+  if (dev_alloc(&c->d_D, n2 * nslot) != cudaSuccess || dev_alloc(&c->d_Ds, n2 * nslot) != cudaSuccess ||
+      dev_alloc(&c->d_Fh, n2 * nslot) != cudaSuccess) {
+    cudaGetLastError();
+    DGF_FAIL(DGF_ERR_NOMEM, "device allocation of density/Fock scratch failed");
+  }
+  c->cap_slots = nslot;
+  if (!c->d_dmax) {
+    if (dev_alloc(&c->d_dmax, (size_t)c->nshell * c->nshell) != cudaSuccess) {
+      cudaGetLastError();
+      DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the density bound failed");
+    }
+  }
+  return DGF_OK;
+}
+
+// Slot preparation: slot s takes density `src` with op 0 = copy, 1 = transpose,
+// 2 = symmetric part, 3 = antisymmetric part; Ds = D_slot + D_slot^T.
+__global__ void prep_slot_kernel(const double *__restrict__ Din, double *__restrict__ D, double *__restrict__ Ds,
+                                 int n, int op) {
+  const int64_t n2 = (int64_t)n * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n2; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = e / n, q = e - p * n;
+    const double a = Din[e], t = Din[q * n + p];
+    double v = (op == 0) ? a : (op == 1) ? t : (op == 2) ? 0.5 * (a + t) : 0.5 * (a - t);
+    D[e] = v;
+    Ds[e] = (op == 3) ? 0.0 : a + t;
+  }
+}
+
+// Output: F = Fh1 + sign * Fh2^T.
+__global__ void combine_kernel(const double *__restrict__ F1, const double *__restrict__ F2, double *__restrict__ F,
+                               int n, double sign) {
+  const int64_t n2 = (int64_t)n * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n2; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = e / n, q = e - p * n;
+    F[e] = F1[e] + sign * F2[q * n + p];
+  }
+}
+
+// Block maxima of |D| per shell pair over all slots (MKDRAO, her2gab.F:1213).
+__global__ void dmax_kernel(const double *__restrict__ D, int nslot, int n, const int *__restrict__ sh_ao,
+                            const int *__restrict__ sh_nf, int ns, float *__restrict__ dm) {
+  const int64_t tot = (int64_t)ns * ns;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int A = (int)(e / ns), B = (int)(e - (int64_t)A * ns);
+    double m = 0.0;
+    for (int s = 0; s < nslot; ++s) {
+      const double *Dk = D + (size_t)s * n * n;
+      for (int i = 0; i < sh_nf[A]; ++i)
+        for (int j = 0; j < sh_nf[B]; ++j) {
+          const int p = sh_ao[A] + i, q = sh_ao[B] + j;
+          m = fmax(m, fmax(fabs(Dk[(size_t)p * n + q]), fabs(Dk[(size_t)q * n + p])));
+        }
+    }
+    dm[e] = (float)m;
+  }
+}
+
+struct SlotSpec {
+  int src, op;
+  double js, ks;
+};
+
+static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double *dmat_dev, double *fmat_dev,
+                     const dgf_options *opt, cudaStream_t st, dgf_stats *stats) {
+  dgf_options o;
+  dgf_default_options(&o);
+  if (opt) o = *opt;
+  if (!(o.thrs >= 0.0)) DGF_FAIL(DGF_ERR_ARG, "thrs must be >= 0");
+  const int N = c->nbf;
+  const size_t n2 = (size_t)N * N;
+  // Decode IFCTYP into density slots and output combinations.
+  std::vector<SlotSpec> slots;
+  struct OutSpec {
+    int s1, s2;
+    double sign;
+    bool zero;
+  };
+  std::vector<OutSpec> outs;
+  for (int k = 0; k < ndmat; ++k) {
+    const int X = (int)(ifctyp[k] / 10), Y0 = (int)(ifctyp[k] % 10);
+    if (X < 0 || X > 2 || Y0 < 1 || Y0 > 3) DGF_FAIL(DGF_ERR_UNSUPPORTED, "unsupported IFCTYP");
+    int Y = Y0;
+    if (X == 2) Y &= 2;                 // antisymmetric density: no Coulomb part
+    if (o.hfxfac == 0.0) Y &= 1;        // no exchange
+    const double js = (Y & 1) ? 1.0 : 0.0, ks = (Y & 2) ? 0.5 * o.hfxfac : 0.0;
+    if (Y == 0) {
+      outs.push_back({0, 0, 0.0, true});
+      continue;
+    }
+    if (X == 1) {
+      slots.push_back({k, 2, js, ks});
+      const int s = (int)slots.size() - 1;
+      outs.push_back({s, s, 1.0, false});
+    } else if (X == 2) {
+      slots.push_back({k, 3, js, ks});
+      const int s = (int)slots.size() - 1;
+      outs.push_back({s, s, -1.0, false});
+    } else {
+      slots.push_back({k, 0, js, ks});
+      slots.push_back({k, 1, js, ks});
+      const int s = (int)slots.size() - 2;
+      outs.push_back({s, s + 1, 1.0, false});
+    }
+  }
+  int st_code = build_plan(c, o.thrs);
+  if (st_code) return st_code;
+  const int nslot_total = (int)slots.size();
+  const int chunk = std::min(kMaxSlots, std::max(nslot_total, 1));
+  st_code = ensure_slots(c, chunk);
+  if (st_code) return st_code;
+  DGF_CUDA_CHECK(cudaMemsetAsync(c->d_cnt, 0, 8 * sizeof(unsigned long long), st));
+  DGF_CUDA_CHECK(cudaEventRecord(c->ev0, st));
+  const bool need_dmax = (o.ifthrs < 20) || (o.mixed_cutoff > 0.0);
+  int64_t launches = 0, total_q = 0;
+  for (const ClassPlan &cp : c->plan) total_q += cp.nquartet;
+  const int eb = 256, eg = (int)std::min<size_t>((n2 + eb - 1) / eb, (size_t)c->nsm * 8);
+  // Zero outputs that have no contributions.
+  for (int k = 0; k < ndmat; ++k)
+    if (outs[k].zero) DGF_CUDA_CHECK(cudaMemsetAsync(fmat_dev + (size_t)k * n2, 0, n2 * 8, st));
+  std::vector<int> sh_nf(c->nshell);
+  int *d_shinfo = nullptr;
+  if (need_dmax) {
+    for (int s = 0; s < c->nshell; ++s) sh_nf[s] = nfun(c->sh_l[s], c->spherical);
+    DGF_CUDA_CHECK(dev_alloc(&d_shinfo, 2 * (size_t)c->nshell));
+    DGF_CUDA_CHECK(cudaMemcpyAsync(d_shinfo, c->sh_ao.data(), c->nshell * 4, cudaMemcpyHostToDevice, st));
+    DGF_CUDA_CHECK(cudaMemcpyAsync(d_shinfo + c->nshell, sh_nf.data(), c->nshell * 4, cudaMemcpyHostToDevice, st));
+  }
+  for (int s0 = 0; s0 < nslot_total; s0 += chunk) {
+    const int ns = std::min(chunk, nslot_total - s0);
+    for (int s = 0; s < ns; ++s) {
+      const SlotSpec &sp = slots[s0 + s];
+      prep_slot_kernel<<<eg, eb, 0, st>>>(dmat_dev + (size_t)sp.src * n2, c->d_D + s * n2, c->d_Ds + s * n2, N,
+                                          sp.op);
+      ++launches;
+    }
+    DGF_CUDA_CHECK(cudaMemsetAsync(c->d_Fh, 0, ns * n2 * 8, st));
+    if (need_dmax) {
+      dmax_kernel<<<std::max(1, std::min(c->nshell * c->nshell / 128 + 1, c->nsm * 8)), 128, 0, st>>>(
+          c->d_D, ns, N, d_shinfo, d_shinfo + c->nshell, c->nshell, c->d_dmax);
+      ++launches;
+    }
+    JKArgs a = base_args(c);
+    a.nslot = ns;
+    a.D = c->d_D;
+    a.Ds = c->d_Ds;
+    a.Fh = c->d_Fh;
+    for (int s = 0; s < ns; ++s) {
+      a.jscale[s] = slots[s0 + s].js;
+      a.kscale[s] = slots[s0 + s].ks;
+    }
+    a.dmax = need_dmax ? c->d_dmax : nullptr;
+    a.dens_thr = (o.ifthrs < 20) ? std::pow(10.0, -(double)o.ifthrs) : 0.0;
+    a.split = o.mixed_cutoff;
+    a.mode = 0;
+    a.counters = c->d_cnt;
+    for (const ClassPlan &cp : c->plan) {
+      a.bra = c->d_pairs + c->cls_off[cp.X];
+      a.ket = c->d_pairs + c->cls_off[cp.Y];
+      a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
+      a.same_class = (cp.X == cp.Y);
+      a.qoff = c->d_qoff + cp.off;
+      a.nquartet = cp.nquartet;
+      // Boys table of order L = la+lb+lc+ld.
+      const int la = (cp.X == 0) ? 0 : (cp.X <= 2) ? 1 : (cp.X <= 5) ? 2 : 3;
+      const int lb = cp.X - la * (la + 1) / 2;
+      const int lc = (cp.Y == 0) ? 0 : (cp.Y <= 2) ? 1 : (cp.Y <= 5) ? 2 : 3;
+      const int ld = cp.Y - lc * (lc + 1) / 2;
+      a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
+      int r = launch_class(c, cp.X, cp.Y, a, st);
+      if (r) {
+        if (d_shinfo) cudaFree(d_shinfo);
+        return r;
+      }
+      ++launches;
+    }
+    // Combine the slots of this chunk into the outputs they belong to.
+    for (int k = 0; k < ndmat; ++k) {
+      const OutSpec &os = outs[k];
+      if (os.zero || os.s1 < s0 || os.s1 >= s0 + ns) continue;
+      combine_kernel<<<eg, eb, 0, st>>>(c->d_Fh + (os.s1 - s0) * n2, c->d_Fh + (os.s2 - s0) * n2,
+                                        fmat_dev + (size_t)k * n2, N, os.sign);
+      ++launches;
+    }
+  }
+  DGF_CUDA_CHECK(cudaGetLastError());
+  DGF_CUDA_CHECK(cudaEventRecord(c->ev1, st));
+  if (d_shinfo) {
+    cudaStreamSynchronize(st);
+    cudaFree(d_shinfo);
+  }
+  if (stats) {
+    unsigned long long cnt[8];
+    DGF_CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    DGF_CUDA_CHECK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    stats->quartets_total = total_q;
+    stats->quartets_fp64 = (int64_t)cnt[0];
+    stats->quartets_fp32 = 0;
+    stats->quartets_skipped = (int64_t)cnt[2];
+    stats->prim_quartets = (int64_t)cnt[1];
+    stats->kernel_launches = launches;
+    stats->ms_device = ms;
+  }
+  return DGF_OK;
+}
+
+static int check_fock_args(dgf_ctx *c, dgf_int ndmat, const dgf_int *ifctyp, const void *d, const void *f) {
+  if (!c) DGF_FAIL(DGF_ERR_ARG, "ctx is NULL");
+  if (ndmat < 0) DGF_FAIL(DGF_ERR_ARG, "ndmat < 0");
+  if (ndmat > 0 && (!ifctyp || !d || !f)) DGF_FAIL(DGF_ERR_ARG, "NULL matrix or IFCTYP array");
+  return DGF_OK;
+}
+
+extern "C" int dgf_fock_device(dgf_ctx *c, dgf_int ndmat, const dgf_int *ifctyp, const double *dmat_device,
+                               double *fmat_device, const dgf_options *opt, void *stream, dgf_stats *stats) {
+  int r = check_fock_args(c, ndmat, ifctyp, dmat_device, fmat_device);
+  if (r || ndmat == 0) return r;
+  DeviceGuard g(c->device);
+  return fock_impl(c, (int)ndmat, ifctyp, dmat_device, fmat_device, opt, (cudaStream_t)stream, stats);
+}
+
+extern "C" int dgf_fock(dgf_ctx *c, dgf_int ndmat, const dgf_int *ifctyp, const double *dmat, double *fmat,
+                        const dgf_options *opt, dgf_stats *stats) {
+  int r = check_fock_args(c, ndmat, ifctyp, dmat, fmat);
+  if (r || ndmat == 0) return r;
+  DeviceGuard g(c->device);
+  const size_t n2 = (size_t)c->nbf * c->nbf;
+  if ((int)ndmat * 2 > c->cap_io) {
+    if (c->d_io) cudaFree(c->d_io);
+    c->d_io = nullptr;
+    c->cap_io = 0;
+    if (dev_alloc(&c->d_io, 2 * ndmat * n2) != cudaSuccess) {
+      cudaGetLastError();
+      DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the D/F staging buffers failed");
+    }
+    c->cap_io = (int)ndmat * 2;
+  }
+  double *dD = c->d_io, *dF = c->d_io + ndmat * n2;
+  DGF_CUDA_CHECK(cudaMemcpyAsync(dD, dmat, ndmat * n2 * 8, cudaMemcpyHostToDevice, c->stream));
+  r = fock_impl(c, (int)ndmat, ifctyp, dD, dF, opt, c->stream, stats);
+  if (r) return r;
+  DGF_CUDA_CHECK(cudaMemcpyAsync(fmat, dF, ndmat * n2 * 8, cudaMemcpyDeviceToHost, c->stream));
+  DGF_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  return DGF_OK;
+}
+
+extern "C" const char *dgf_strerror(int s) {
+  switch (s) {
+    case DGF_OK: return "success";
+    case DGF_ERR_ARG: return "invalid argument";
+    case DGF_ERR_NOMEM: return "out of memory";
+    case DGF_ERR_CUDA: return "CUDA runtime error";
+    case DGF_ERR_UNSUPPORTED: return "unsupported angular momentum, IFCTYP or option";
+    case DGF_ERR_TIMEOUT: return "bounded device wait timed out";
+    case DGF_ERR_NODEVICE: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char *dgf_last_error(void) { return dgf::g_last_error.c_str(); }

@@ -1,0 +1,118 @@
+// Internal definitions shared by the host runtime and the device kernels of
+// libdgfock (the B200 direct J/K Fock build).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/dgfock.h"
+
+namespace dgf {
+
+constexpr int kMaxShellL = 3;                                         // s, p, d, f
+constexpr int kNumPairClass = (kMaxShellL + 1) * (kMaxShellL + 2) / 2;  // (la >= lb) classes
+constexpr int kMaxSlots = 8;  // density slots processed together by one kernel pass
+
+// Boys-function table: F_M(T) on [0, kBoysTmax) in kBoysNint intervals of
+// width 1/kBoysPerUnit, a degree-kBoysDeg polynomial in x = (T - mid) * 2 *
+// kBoysPerUnit per interval (Chebyshev interpolant converted to powers of x).
+constexpr int kBoysMaxM = 17;
+constexpr int kBoysPerUnit = 2;
+constexpr double kBoysTmax = 40.0;
+constexpr int kBoysNint = 80;
+constexpr int kBoysDeg = 11;
+constexpr int kBoysNcoef = kBoysDeg + 1;
+constexpr int kBoysTableDoubles = kBoysNint * kBoysNcoef;
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int n3(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }
+__host__ __device__ constexpr int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// Primitive pair of a shell pair (A first, the higher angular momentum).
+// K = c_a c_b exp(-mu |AB|^2) sqrt(2 pi^(5/2)) / p, Dalton's FAC12 with R2PI52
+// (DALTON/abacus/her2odc.F:229-231, DALTON/include/pi.h:9-14).
+struct PrimPair {
+  double p, Px, Py, Pz, PAx, PAy, PAz, PBx, PBy, PBz, K, pad;
+};
+
+// Shell pair record in a class list (sorted by Schwarz factor, descending).
+struct PairRec {
+  int shA, shB;    // segmented shell indices (A has l >= l of B)
+  int aoA, aoB;    // first AO of each shell
+  int pp0, npp;    // primitive-pair range
+  int same;        // A == B
+  int atA;         // atom of A (atom of B in atB)
+  int atB, pad;
+  double Q;        // Schwarz factor sqrt(max |(ab|ab)|)
+};
+
+// Arguments of one quartet-class launch.
+struct JKArgs {
+  const PairRec *bra;
+  const PairRec *ket;
+  const int64_t *qoff;      // prefix sums of ket partners per bra (nbra+1), device
+  int nbra;
+  int same_class;           // bra class == ket class (canonical ket <= bra)
+  int64_t nquartet;
+  const PrimPair *pp;
+  const double *boys;       // table for M = L of this class
+  const double *sph;        // Cartesian->spherical tables, see sph_offset()
+  int spherical;
+  int nbf;
+  int nslot;
+  const double *D;          // [nslot][N*N] densities (exchange)
+  const double *Ds;         // [nslot][N*N] D + D^T (Coulomb)
+  double *Fh;               // [nslot][N*N] half Fock accumulators
+  double jscale[kMaxSlots];
+  double kscale[kMaxSlots];
+  // screening / precision split
+  const float *dmax;        // [nshell*nshell] max |D| per shell pair, or null
+  int nshell;
+  double dens_thr;          // skip if bound < dens_thr (0: no density screening)
+  double split;             // precision split bound
+  int mode;                 // 0: all, 1: bound >= split only, 2: bound < split only
+  double *diag_out;         // Schwarz mode: sqrt(max |(ab|ab)|) per bra pair, no digestion
+  unsigned long long *counters;  // [0] quartets done, [1] primitive quartets, [2] skipped
+};
+
+// Offset of the l-block of the Cartesian->spherical table: rows m=-l..l,
+// ncart(l) columns, l = 0..kMaxShellL+1.
+__host__ __device__ inline int sph_offset(int l) {
+  int off = 0;
+  for (int k = 0; k < l; ++k) off += (2 * k + 1) * ncart(k);
+  return off;
+}
+constexpr int kSphTableDoubles = 1 * 1 + 3 * 3 + 5 * 6 + 7 * 10 + 9 * 15;
+
+typedef void (*JKLauncher)(const JKArgs &, int grid, int block, size_t smem, cudaStream_t);
+
+struct ClassKernel {
+  JKLauncher launch;
+  int block;
+  size_t smem;
+};
+
+// Per-class launch table (filled by dgf_jk.cu): index [X][Y] of pair classes.
+const ClassKernel &jk_kernel(int X, int Y, int precision);
+cudaError_t jk_prepare_all();
+
+void boys_table_host(std::vector<double> &out);       // [kBoysMaxM+1][kBoysTableDoubles]
+void sph_table_host(std::vector<double> &out);        // kSphTableDoubles
+double boys_reference(int m, double t);               // accurate host F_m(t)
+
+void set_error(const char *file, int line, const std::string &msg);
+
+}  // namespace dgf
+
+#define DGF_CUDA_CHECK(expr)                                                   \
+  do {                                                                         \
+    cudaError_t _e = (expr);                                                   \
+    if (_e != cudaSuccess) {                                                   \
+      ::dgf::set_error(__FILE__, __LINE__, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+      return DGF_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)

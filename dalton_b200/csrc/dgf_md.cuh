@@ -1,0 +1,105 @@
+// Device building blocks of the McMurchie-Davidson quartet kernels:
+// Boys function from the shared-memory table, Hermite expansion
+// coefficients, index helpers.  Shared by the Fock, Schwarz and gradient
+// kernels.
+#pragma once
+
+#include "dgf_internal.h"
+
+namespace dgf {
+
+__host__ __device__ constexpr int nfun(int l, int spherical) { return (spherical && l >= 2) ? 2 * l + 1 : ncart(l); }
+
+// Compact index of (t,u,v) with t+u+v = s: s-major, then u+v, then v.
+__host__ __device__ __forceinline__ int tuv_index(int t, int u, int v) {
+  int s = t + u + v, w = u + v;
+  return s * (s + 1) * (s + 2) / 6 + w * (w + 1) / 2 + v;
+}
+
+// Inverse of tuv_index.
+__host__ __device__ __forceinline__ void tuv_decode(int e, int &t, int &u, int &v) {
+  int s = 0;
+  while (n3(s) <= e) ++s;
+  int r = e - s * (s + 1) * (s + 2) / 6;
+  int w = 0;
+  while ((w + 1) * (w + 2) / 2 <= r) ++w;
+  v = r - w * (w + 1) / 2;
+  u = w - v;
+  t = s - w;
+}
+
+// Cartesian exponents of component k of shell l in Dalton order
+// (xx, xy, xz, yy, yz, zz): k = s(s+1)/2 + z with s = y + z.
+__host__ __device__ __forceinline__ void cart_decode(int l, int k, int &x, int &y, int &z) {
+  int s = 0;
+  while ((s + 1) * (s + 2) / 2 <= k) ++s;
+  z = k - s * (s + 1) / 2;
+  y = s - z;
+  x = l - s;
+}
+
+// F_0..F_M(T): table polynomial for F_M below kBoysTmax then downward
+// recursion F_m = (2T F_{m+1} + e^-T)/(2m+1); above it F_0 = sqrt(pi/T)/2
+// and upward recursion F_{m+1} = ((2m+1) F_m - e^-T)/(2T).
+template <int M>
+__device__ __forceinline__ void boys_eval(double T, const double *__restrict__ tab, double *F) {
+  if (T < kBoysTmax) {
+    int i = (int)(T * kBoysPerUnit);
+    double x = (T - (i + 0.5) * (1.0 / kBoysPerUnit)) * (2.0 * kBoysPerUnit);
+    const double *c = tab + i * kBoysNcoef;
+    double f = c[kBoysDeg];
+#pragma unroll
+    for (int k = kBoysDeg - 1; k >= 0; --k) f = fma(f, x, c[k]);
+    F[M] = f;
+    if (M > 0) {
+      double et = exp(-T), t2 = 2.0 * T;
+#pragma unroll
+      for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], et) * (1.0 / (2 * m + 1));
+    }
+  } else {
+    double rt = rsqrt(T);
+    F[0] = 0.88622692545275801364908374167057 * rt;
+    if (M > 0) {
+      double et = exp(-T), h = 0.5 * rt * rt;
+#pragma unroll
+      for (int m = 0; m < M; ++m) F[m + 1] = fma((double)(2 * m + 1), F[m], -et) * h;
+    }
+  }
+}
+
+// Hermite expansion coefficients of one direction, E^{ij}_t for i <= LA,
+// j <= LB, t <= i+j, E^{00}_0 = 1; layout E[(i*(LB+1)+j)*(LA+LB+1)+t].
+// h = 1/(2p).  SIGN = -1 multiplies E_t by (-1)^t (ket side of the MD sum).
+template <int LA, int LB, int SIGN, typename T>
+__device__ __forceinline__ void herm_e(T h, T pa, T pb, T *E) {
+  constexpr int NT = LA + LB + 1;
+#pragma unroll
+  for (int k = 0; k < (LA + 1) * (LB + 1) * NT; ++k) E[k] = T(0);
+  E[0] = T(1);
+#pragma unroll
+  for (int i = 0; i <= LA; ++i) {
+#pragma unroll
+    for (int j = 0; j <= LB; ++j) {
+      if (i == 0 && j == 0) continue;
+      const int pi = (i > 0) ? i - 1 : 0, pj = (i > 0) ? j : j - 1;
+      const T x = (i > 0) ? pa : pb;
+      const int top = pi + pj;
+      const T *prev = E + (pi * (LB + 1) + pj) * NT;
+      T *cur = E + (i * (LB + 1) + j) * NT;
+#pragma unroll
+      for (int t = 0; t <= i + j; ++t) {
+        T v = (t <= top) ? x * prev[t] : T(0);
+        if (t > 0) v += h * prev[t - 1];
+        if (t + 1 <= top) v += T(t + 1) * prev[t + 1];
+        cur[t] = v;
+      }
+    }
+  }
+  if (SIGN < 0) {
+#pragma unroll
+    for (int k = 0; k < (LA + 1) * (LB + 1) * NT; ++k)
+      if ((k % NT) & 1) E[k] = -E[k];
+  }
+}
+
+}  // namespace dgf

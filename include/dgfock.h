@@ -1,0 +1,152 @@
+/* dgfock — B200-native direct J/K Fock build, C ABI.
+ *
+ * Drop-in for the two-electron Fock call of Dalton's SCF:
+ *   SUBROUTINE HERFCK(FMAT,DMAT,NDMT,ISYMDM,IFCTYP,IPRFCK,WORK,LWORK)
+ *   (DALTON/abacus/herdirect.F:431-551), reached from SIRFCK
+ *   (DALTON/sirius/sirfck.F:387) and from FCK2AO (DALTON/sirius/sirgrad.F:714).
+ *
+ * Contract kept from HERFCK:
+ *   - FMAT(N,N,NDMT) is overwritten (HERFCK_1 zeroes it, herdirect.F:686);
+ *     DMAT(N,N,NDMT) is read only.  Matrices are full squares in Dalton's C1
+ *     AO order; a symmetric matrix reads the same in C (row-major) and
+ *     Fortran (column-major) order, and general ones are documented per call.
+ *   - IFCTYP = 10*X + Y per matrix (sirfck.F:45-57): X = 1 symmetric,
+ *     0 general, 2 antisymmetric density; Y = 1 Coulomb, 2 exchange, 3 both.
+ *     F = [Y&1] J[D] - [Y&2] (hfxfac/2) K[D] with
+ *       J_pq = sum_rs (pq|rs) D_rs,   K_pq = sum_rs (pr|qs) D_rs
+ *     (FCKD03, sirfck.F:1496-1547; FCKCON, herfckcon.F:20-220).
+ *   - Shell quartets with Q_AB*Q_CD < thrs are skipped (Schwarz, THRS
+ *     default 1e-12, herrdn.F:359; her2gab.F GABGEN); with ifthrs < 20 also
+ *     those with Q_AB*Q_CD*max(4|D|_Coulomb, |D|_exchange) < 10^-ifthrs
+ *     (SYMLOP screening, her2drv.F:2663-2733).
+ *   - Errors are returned as status codes (0 = success), never by aborting;
+ *     the Fortran shim maps a nonzero status to QUIT (gptrygve.F:256).
+ *
+ * All pointers are host pointers unless a name says _device.  A context is
+ * not thread-safe; separate contexts are independent.
+ */
+#ifndef DGFOCK_H
+#define DGFOCK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Integer width of the ABI.  Dalton is built with 4-byte INTEGER unless
+ * -DVAR_INT64 (cmake/Definitions.cmake:30); this library takes int64 and a
+ * 4-byte-INTEGER Dalton widens its arrays in the shim. */
+typedef int64_t dgf_int;
+
+typedef struct dgf_ctx dgf_ctx;
+
+/* Status codes. */
+enum {
+  DGF_OK = 0,
+  DGF_ERR_ARG = 1,         /* invalid argument */
+  DGF_ERR_NOMEM = 2,       /* device or host allocation failed */
+  DGF_ERR_CUDA = 3,        /* CUDA runtime error */
+  DGF_ERR_UNSUPPORTED = 4, /* angular momentum, IFCTYP or option not supported */
+  DGF_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  DGF_ERR_NODEVICE = 6     /* no CUDA device / extension unusable */
+};
+
+/* Basis in Dalton block form (one block = one atom's shell of angular
+ * momentum l: nprim primitives shared by ncontr contracted functions, CPRIM
+ * coefficients already normalised as NRMORB does, herrdn.F:3263-3290).
+ * AO offsets follow Dalton's C1 order: atom -> l -> contraction -> component
+ * (p as x,y,z; d and higher as real spherical m=-l..l when spherical=1,
+ * SPHCOM MINTEG=2, her1pro.F:4671-4790; Cartesian xx,xy,xz,yy,yz,zz,...
+ * otherwise).  This is what a Fortran shim gathers from /SHELLS/ and
+ * /PRIMIT/. */
+typedef struct {
+  dgf_int nblock, natom, nbf, spherical;
+  const dgf_int *block_l, *block_atom, *block_nprim, *block_ncontr;
+  const dgf_int *block_ao_offset, *block_prim_offset, *block_coef_offset;
+  const double *prim_exp;   /* concatenated exponents */
+  const double *coef;       /* per block, column-major (nprim, ncontr) */
+  const double *atom_xyz;   /* (natom, 3) bohr */
+  const double *atom_charge;/* (natom) nuclear charges */
+} dgf_basis;
+
+/* Work counters of one call (HERFCK's DINTSKP/SCRSTA statistics,
+ * her2drv.F:495-541, her2gab.F:1486, in this library's units). */
+typedef struct {
+  int64_t quartets_total;    /* canonical shell quartets with Q_AB*Q_CD >= thrs */
+  int64_t quartets_fp64;     /* evaluated in FP64 */
+  int64_t quartets_fp32;     /* evaluated in FP32 (mixed form) */
+  int64_t quartets_skipped;  /* skipped by density screening */
+  int64_t prim_quartets;     /* primitive quartets evaluated */
+  int64_t kernel_launches;   /* device kernels launched by the call */
+  double ms_device;          /* device time of the Fock build (CUDA events) */
+} dgf_stats;
+
+/* Fock-build options (no globals; Dalton's COMMON values passed in).
+ * thrs: Schwarz threshold (THRS, 1e-12 default);
+ * ifthrs: density screening exponent (>= 20 disables, HR2INP .IFTHRS);
+ * hfxfac: exchange factor (HFXFAC, 1 for HF);
+ * mixed_cutoff: 0 = all-FP64 drop-in; > 0 = quartets whose bound
+ *   Q_AB*Q_CD*Dmax is below it are evaluated in FP32 (Boys function,
+ *   accumulation and digestion stay FP64). */
+typedef struct {
+  double thrs;
+  dgf_int ifthrs;
+  double hfxfac;
+  double mixed_cutoff;
+} dgf_options;
+
+/* Default options: thrs 1e-12, ifthrs 20, hfxfac 1, mixed_cutoff 0. */
+void dgf_default_options(dgf_options *opt);
+
+/* Create a context on CUDA device `device`: copies the basis to the device,
+ * builds the shell-pair records, Schwarz factors and class-sorted pair lists
+ * (the GETGAB/GABGEN pre-pass, her2gab.F:1776-1928, once per geometry). */
+int dgf_create(const dgf_basis *basis, int device, dgf_ctx **out);
+
+/* Free a context (and all its device memory). NULL is ignored. */
+void dgf_destroy(dgf_ctx *ctx);
+
+/* HERFCK: F(N,N,ndmat) from D(N,N,ndmat), host pointers.  Replaces the
+ * HERFCK_1 / ERIFCK dispatch (herdirect.F:514-553).  stats may be NULL. */
+int dgf_fock(dgf_ctx *ctx, dgf_int ndmat, const dgf_int *ifctyp, const double *dmat, double *fmat,
+             const dgf_options *opt, dgf_stats *stats);
+
+/* Same with device pointers, enqueued on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream); no host synchronisation except what screening
+ * set-up needs.  dmat_device/fmat_device hold ndmat N*N doubles. */
+int dgf_fock_device(dgf_ctx *ctx, dgf_int ndmat, const dgf_int *ifctyp, const double *dmat_device,
+                    double *fmat_device, const dgf_options *opt, void *stream, dgf_stats *stats);
+
+/* Two-electron part of the RHF nuclear gradient (TWOEXP -> INTEX1 -> DEROUT,
+ * aba2tex.F:242, her2ave.F:91-830): grad(natom,3) is overwritten with
+ *   1/2 sum_pqrs d(pq|rs)/dx [D_pq D_rs - hfxfac/2 D_pr D_qs],
+ * D the symmetric total density (host pointers). */
+int dgf_grad2e(dgf_ctx *ctx, const double *dmat, double hfxfac, double thrs, double *grad);
+
+/* Device-pointer form of dgf_grad2e. */
+int dgf_grad2e_device(dgf_ctx *ctx, const double *dmat_device, double hfxfac, double thrs, double *grad_device,
+                      void *stream);
+
+/* One-electron integrals S, T, V (N x N each, host pointers, any may be
+ * NULL): the HER1 integrals the SCF host needs next to the Fock build. */
+int dgf_oneint(dgf_ctx *ctx, double *S, double *T, double *V);
+
+/* One-electron + nuclear-repulsion part of the RHF gradient:
+ * sum D_pq dh_pq/dx - sum W_pq dS_pq/dx + dVnn/dx, grad(natom,3). */
+int dgf_grad1e(dgf_ctx *ctx, const double *dmat, const double *wmat, double *grad);
+
+/* Number of basis functions, atoms and segmented shells of a context. */
+int dgf_info(const dgf_ctx *ctx, dgf_int *nbf, dgf_int *natom, dgf_int *nshell);
+
+/* Message text of a status code. */
+const char *dgf_strerror(int status);
+
+/* Text of the last error recorded on this thread (file/line and CUDA text). */
+const char *dgf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGFOCK_H */

@@ -427,6 +427,19 @@ void orc_sph_matrix(int l, double *out) {
 
 int orc_nshell(const orc_basis *b) { return (int)make_basis(b).sh.size(); }
 
+int orc_schwarz(const orc_basis *b, double *q, int64_t *shell_l, int64_t *shell_nprim, int64_t *shell_atom) {
+  set_threads();
+  Basis B = make_basis(b);
+  std::vector<double> Q = schwarz(B);
+  std::memcpy(q, Q.data(), Q.size() * sizeof(double));
+  for (size_t i = 0; i < B.sh.size(); ++i) {
+    shell_l[i] = B.sh[i].l;
+    shell_nprim[i] = B.sh[i].nprim;
+    shell_atom[i] = B.sh[i].atom;
+  }
+  return 0;
+}
+
 int orc_eri_full(const orc_basis *b, double *eri) {
   set_threads();
   Basis B = make_basis(b);

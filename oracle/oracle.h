@@ -48,6 +48,8 @@ int orc_eri_full(const orc_basis *b, double *eri);
 /* Schwarz factors per segmented shell pair: Q_AB = sqrt(max |(ab|ab)|).
  * Returns the number of segmented shells in *nshell. */
 int orc_nshell(const orc_basis *b);
+int orc_schwarz(const orc_basis *b, double *q /* nshell^2 */, int64_t *shell_l, int64_t *shell_nprim,
+                int64_t *shell_atom);
 
 /* Fock build with HERFCK semantics (FMAT overwritten):
  *   IFCTYP = 10*X + Y; X = 1 symmetric D, 0 general, 2 antisymmetric;

@@ -51,6 +51,7 @@ def lib():
         _lib.orc_sph_matrix.argtypes = [ctypes.c_int, _dp]
         _lib.orc_set_threads.argtypes = [ctypes.c_int]
         _lib.orc_nshell.argtypes = [ctypes.POINTER(OrcBasis)]
+        _lib.orc_schwarz.argtypes = [ctypes.POINTER(OrcBasis), _dp, _i64p, _i64p, _i64p]
     return _lib
 
 
@@ -102,6 +103,17 @@ def sph_matrix(l: int) -> np.ndarray:
 def nshell(bs) -> int:
     h = _Holder(bs)
     return lib().orc_nshell(ctypes.byref(h.s))
+
+
+def schwarz(bs):
+    """Schwarz factors of the segmented shells: (Q (ns,ns), l (ns,), nprim (ns,), atom (ns,))."""
+    h = _Holder(bs)
+    ns = lib().orc_nshell(ctypes.byref(h.s))
+    q = np.zeros((ns, ns))
+    l, n, a = (np.zeros(ns, dtype=np.int64) for _ in range(3))
+    lib().orc_schwarz(ctypes.byref(h.s), _p(q, ctypes.c_double), _p(l, ctypes.c_int64), _p(n, ctypes.c_int64),
+                      _p(a, ctypes.c_int64))
+    return q, l, n, a
 
 
 def oneint(bs):
