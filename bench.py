@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of the direct J+K Fock build (libdgfock) on B200.
+
+Workload (default): (H2O)32 water cluster, cc-pVDZ, 768 spherical basis
+functions, closed-shell RHF density after a 12-iteration SCF.  A step is one
+J+K build (IFCTYP 13, Schwarz 1e-12) of that density.  Both the all-FP64
+drop-in and the mixed form (quartets with Q_AB Q_CD |D| < 1e-6 contracted in
+FP32) are timed; the headline value is the mixed form when its energy error
+against the FP64 build is within 1e-6 Eh, else the FP64 form.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun (N > 1) each rank evaluates 1/N of every class's quartet
+queue and the partial Fock matrices are summed with an NCCL all-reduce inside
+the timed step (strong scaling: the molecule is fixed).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "J+K build ms & ERI quartets/s, mixed vs FP64 at <=1e-6 Eh; HF gradient ms"
+MIXED_CUTOFF = 1e-6
+THRS = 1e-12
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dgfock", choices=["dgfock", "reference"])
+    ap.add_argument("--workload", default="h2o32_ccpvdz")
+    ap.add_argument("--scf-iters", type=int, default=12)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample time")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only run warmup+steps builds of a core-guess density (for ncu captures)")
+    ap.add_argument("--mixed", action="store_true", help="with --profile-run: mixed form")
+    return ap.parse_args()
+
+
+def profile_run(args):
+    """Minimal driver for profiler captures: W+K J+K builds, no SCF, no timing."""
+    import torch
+
+    from dalton_b200 import molecules
+    from dalton_b200.basis import build_basis
+    from dalton_b200.fock import FockBuilder
+
+    mol, basis = molecules.config(args.workload)
+    bs = build_basis(mol, basis)
+    fb = FockBuilder(bs)
+    S, T, V = fb.oneint()
+    Hm = torch.tensor(T + V, device="cuda")
+    Sm = torch.tensor(S, device="cuda")
+    s, U = torch.linalg.eigh(Sm)
+    X = U / torch.sqrt(s)
+    e, C = torch.linalg.eigh(X.T @ Hm @ X)
+    C = X @ C
+    nocc = mol.nelectrons() // 2
+    D = (2.0 * C[:, :nocc] @ C[:, :nocc].T).contiguous()
+    for _ in range(args.warmup + args.steps):
+        fb.herfck_device(D, ifctyp=13, thrs=THRS, mixed_cutoff=MIXED_CUTOFF if args.mixed else 0.0)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_run": args.workload, "builds": args.warmup + args.steps, "stats": fb.last_stats}))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_sample(bs, dmat, target_s, threads=0):
+    """Oracle (CPU restatement of Dalton's HERMIT J+K) on every stride-th bra
+    pair of the same workload, sized to ~target_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+
+    orc.build()
+    if threads:
+        orc.set_threads(threads)
+    cores = orc.threads()
+    t0 = time.perf_counter()
+    orc.fock_sampled(bs, dmat, 1 << 30, 0, THRS)  # set-up only (Schwarz pre-pass)
+    overhead = time.perf_counter() - t0
+    stride = 4000
+    t0 = time.perf_counter()
+    _, nq = orc.fock_sampled(bs, dmat, stride, 0, THRS)
+    dt = max(time.perf_counter() - t0 - overhead, 1e-3)
+    rate = nq / dt
+    total_pairs_frac = 1.0 / stride
+    # second, larger sample sized to the target time
+    want_q = rate * target_s
+    stride2 = max(1, int(nq * stride / max(want_q, 1.0)))
+    if stride2 < stride:
+        t0 = time.perf_counter()
+        _, nq = orc.fock_sampled(bs, dmat, stride2, 0, THRS)
+        dt = max(time.perf_counter() - t0 - overhead, 1e-3)
+        rate = nq / dt
+        total_pairs_frac = 1.0 / stride2
+    return {"value": rate, "unit": "quartets/s", "cores": cores, "kind": "port",
+            "sample": f"oracle J+K (CPU restatement of Dalton HERMIT; Dalton itself needs gfortran, absent) on "
+                      f"every {int(round(1 / total_pairs_frac))}-th bra shell pair of the same workload: "
+                      f"{nq} quartets in {dt:.2f} s (Schwarz pre-pass excluded)",
+            "seconds": dt, "quartets": nq}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    from dalton_b200.basis import build_basis
+    from dalton_b200 import molecules
+
+    mol, basis = molecules.config(args.workload)
+    bs = build_basis(mol, basis)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+
+    orc.build()
+    # A fixed, physically shaped density: the oracle's SCF is too slow at this
+    # size, so use a superposition-of-monomers guess (same quartet set: the
+    # Schwarz screen does not depend on D).
+    rng = np.random.default_rng(0)
+    d = rng.normal(size=(bs.nbf, bs.nbf)) * 1e-3
+    d = d + d.T + np.eye(bs.nbf) * 0.5
+    per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
+    vals = []
+    info = None
+    for k in range(args.warmup + args.steps):
+        info = cpu_baseline_sample(bs, d, per_step)
+        if k >= args.warmup:
+            vals.append(info["value"])
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "quartets/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {mol.natom} atoms, {basis}, {bs.nbf} basis functions, "
+                                   f"J+K IFCTYP 13, Schwarz {THRS}", "cpu_sample_per_step_s": per_step},
+            "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": info["cores"], "kind": "port",
+                             "sample": info["sample"]},
+            "e2e": {"value": v, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.profile_run:
+        profile_run(args)
+        return
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    world, rank, local = dist_setup(args)
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (libdgfock has no CPU path)")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    from dalton_b200 import molecules
+    from dalton_b200.basis import build_basis
+    from dalton_b200.fock import FockBuilder
+    from dalton_b200.perfmodel import class_flops
+    from dalton_b200.scf import rhf
+    from dalton_b200 import _lib
+
+    mol, basis = molecules.config(args.workload)
+    bs = build_basis(mol, basis)
+    fb = FockBuilder(bs, device=local)
+    shard = (rank, world)
+
+    def build(D, mixed, out=None):
+        F = fb.herfck_device(D, fmat=out, ifctyp=13, thrs=THRS, mixed_cutoff=MIXED_CUTOFF if mixed else 0.0,
+                             shard=shard)
+        if pg is not None:
+            pg.all_reduce(F)
+        return F
+
+    # Density: 12-iteration RHF with the FP64 builds (replicated on every rank).
+    t0 = time.perf_counter()
+    scf64 = rhf(bs, fb, maxiter=args.scf_iters, fixed_iterations=args.scf_iters, thrs=THRS)
+    scf_mix = rhf(bs, fb, maxiter=args.scf_iters, fixed_iterations=args.scf_iters, thrs=THRS,
+                  mixed_cutoff=MIXED_CUTOFF)
+    scf_s = time.perf_counter() - t0
+    D = scf64["dmat"].contiguous()
+    H = scf64["H"]
+    enuc = scf64["enuc"]
+    # Accuracy of the mixed build at the converged density.
+    F64 = build(D, False).clone()
+    Fmx = build(D, True).clone()
+    e64 = float(0.5 * torch.sum(D * (2 * H + F64))) + enuc
+    emx = float(0.5 * torch.sum(D * (2 * H + Fmx))) + enuc
+    dE = abs(emx - e64)
+    dF = float(torch.max(torch.abs(Fmx - F64)))
+    mixed_ok = dE <= 1e-6
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+    Fout = torch.empty_like(D)
+
+    def timed(mixed, steps, warmup):
+        for _ in range(warmup):
+            build(D, mixed, Fout)
+        torch.cuda.synchronize(dev)
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize(dev)
+        total = 0.0
+        launches = 0
+        quartets = 0
+        for _ in range(steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            build(D, mixed, Fout)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+            launches += int(fb.last_stats.get("kernel_launches", 0))
+            quartets += int(fb.last_stats.get("quartets_total", 0))
+        torch.cuda.synchronize(dev)
+        ms = total / steps
+        if pg is not None:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            q = torch.tensor([quartets], device=dev, dtype=torch.float64)
+            pg.all_reduce(q)
+            ms, quartets = float(t), int(q)
+        return ms, quartets / steps, launches
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms64, q64, l64 = timed(False, args.steps, args.warmup)
+    msmx, qmx, lmx = timed(True, args.steps, args.warmup)
+    clk = clocks.stop()
+    headline_mixed = mixed_ok
+    ms = msmx if headline_mixed else ms64
+    quartets = qmx if headline_mixed else q64
+    value = quartets / (ms * 1e-3)
+
+    # End to end through the host-pointer C ABI (pinned host D in, host F out).
+    Dh = torch.empty(D.shape, dtype=torch.float64, pin_memory=True)
+    Dh.copy_(D)
+    Fh = torch.empty(D.shape, dtype=torch.float64, pin_memory=True)
+    d_np, f_np = Dh.numpy(), Fh.numpy()
+    for _ in range(args.warmup):
+        f_np[...] = fb.herfck(d_np, 13, thrs=THRS, mixed_cutoff=MIXED_CUTOFF if headline_mixed else 0.0, shard=shard)
+    e2e_total = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        if pg is not None:
+            pg.barrier()
+        t0 = time.perf_counter()
+        f_np[...] = fb.herfck(d_np, 13, thrs=THRS, mixed_cutoff=MIXED_CUTOFF if headline_mixed else 0.0,
+                              shard=shard)
+        if pg is not None:
+            Fdev = torch.from_numpy(f_np).to(dev)
+            pg.all_reduce(Fdev)
+            Fh.copy_(Fdev)
+        e2e_total += time.perf_counter() - t0
+    e2e_ms = e2e_total / args.steps * 1e3
+    if pg is not None:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t)
+    nbytes = D.numel() * 8
+
+    # Roofline of the dominant class kernel (profiled build, same stream).
+    fb.set_profiling(True)
+    build(D, headline_mixed, Fout)
+    prof = fb.profile()
+    fb.set_profiling(False)
+    fp64_peak, fp32_peak = _lib.measure_fma_peak(local)
+    by_time = sorted(prof, key=lambda r: -r["ms"])
+    top = by_time[0]
+    top_flops = class_flops(top["la"], top["lb"], top["lc"], top["ld"], top["prim_quartets"], top["evaluated"])
+    achieved = top_flops / (top["ms"] * 1e-3) / 1e12
+    peak = fp64_peak if top["precision"] == 64 else fp32_peak
+    tot_ms = sum(r["ms"] for r in prof)
+    roofline = {"bound": "fp64" if top["precision"] == 64 else "fp32",
+                "kernel": f"jk_{'thread' if top['kernel'] == 0 else 'team'}_kernel<{top['la']},{top['lb']},"
+                          f"{top['lc']},{top['ld']},{'double' if top['precision'] == 64 else 'float'}>",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "measured FMA-loop peak on this GPU (MEASURED_PEAKS.json has no FP64 figure)",
+                "traffic": None, "share_of_build": top["ms"] / tot_ms if tot_ms else None,
+                "flops_model": "dalton_b200/perfmodel.py (per primitive and per contracted quartet)"}
+    all_flops = sum(class_flops(r["la"], r["lb"], r["lc"], r["ld"], r["prim_quartets"], r["evaluated"]) for r in prof)
+    build_tflops = all_flops / (tot_ms * 1e-3) / 1e12 if tot_ms else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(bs, D.cpu().numpy(), args.cpu_seconds)
+        cpu.pop("seconds", None)
+        cpu.pop("quartets", None)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64+f32 (mixed)" if headline_mixed else "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: (H2O)32 cluster (seeded), {basis}, {bs.nbf} spherical basis "
+                                   f"functions, J+K IFCTYP 13, Schwarz {THRS}, RHF density after "
+                                   f"{args.scf_iters} SCF iterations",
+                       "mixed_cutoff": MIXED_CUTOFF, "parallelism": f"quartet-queue shards x{world}",
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "fp64": {"ms": ms64, "quartets_per_s": q64 / (ms64 * 1e-3), "quartets": q64},
+            "mixed": {"ms": msmx, "quartets_per_s": qmx / (msmx * 1e-3), "quartets": qmx,
+                      "energy_error_Eh": dE, "max_abs_dF": dF, "speedup_vs_fp64": ms64 / msmx},
+            "scf": {"iterations": args.scf_iters, "energy_fp64": scf64["energy"], "energy_mixed_incremental":
+                    scf_mix["energy"], "energy_diff_Eh": abs(scf_mix["energy"] - scf64["energy"]),
+                    "seconds_both": scf_s},
+            "e2e": {"value": quartets / (e2e_ms * 1e-3), "unit": "quartets/s", "ms": e2e_ms,
+                    "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+            "roofline": roofline, "build_tflops_model": build_tflops,
+            "peaks_measured": {"fp64_tflops": fp64_peak, "fp32_tflops": fp32_peak},
+            "gpu_launches": int((lmx if headline_mixed else l64)),
+            "clocks": clk, "cpu_baseline": cpu,
+            "profile_top": [{k: r[k] for k in ("la", "lb", "lc", "ld", "precision", "kernel", "evaluated",
+                                               "prim_quartets", "ms")} for r in by_time[:8]],
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    fb.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -19,7 +19,8 @@ DGF_OK, DGF_ERR_ARG, DGF_ERR_NOMEM, DGF_ERR_CUDA, DGF_ERR_UNSUPPORTED, DGF_ERR_T
 
 # Every symbol include/dgfock.h declares.
 EXPORTS = ["dgf_default_options", "dgf_create", "dgf_destroy", "dgf_fock", "dgf_fock_device", "dgf_grad2e",
-           "dgf_grad2e_device", "dgf_oneint", "dgf_grad1e", "dgf_info", "dgf_strerror", "dgf_last_error"]
+           "dgf_grad2e_device", "dgf_oneint", "dgf_grad1e", "dgf_set_profiling", "dgf_get_profile",
+           "dgf_measure_fma_peak", "dgf_info", "dgf_strerror", "dgf_last_error"]
 
 
 class DgfBasis(ctypes.Structure):
@@ -31,7 +32,7 @@ class DgfBasis(ctypes.Structure):
 
 class DgfOptions(ctypes.Structure):
     _fields_ = [("thrs", ctypes.c_double), ("ifthrs", dgf_int), ("hfxfac", ctypes.c_double),
-                ("mixed_cutoff", ctypes.c_double)]
+                ("mixed_cutoff", ctypes.c_double), ("shard_index", dgf_int), ("shard_count", dgf_int)]
 
 
 class DgfStats(ctypes.Structure):
@@ -39,6 +40,15 @@ class DgfStats(ctypes.Structure):
                 ("quartets_fp32", ctypes.c_int64), ("quartets_skipped", ctypes.c_int64),
                 ("prim_quartets", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
                 ("ms_device", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class DgfClassTime(ctypes.Structure):
+    _fields_ = [("la", ctypes.c_int32), ("lb", ctypes.c_int32), ("lc", ctypes.c_int32), ("ld", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("kernel", ctypes.c_int32), ("quartets", ctypes.c_int64),
+                ("evaluated", ctypes.c_int64), ("prim_quartets", ctypes.c_int64), ("ms", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -75,6 +85,9 @@ def load() -> ctypes.CDLL:
     lib.dgf_oneint.argtypes = [vp, _dp, _dp, _dp]
     lib.dgf_grad1e.argtypes = [vp, _dp, _dp, _dp]
     lib.dgf_info.argtypes = [vp, _ip, _ip, _ip]
+    lib.dgf_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.dgf_get_profile.argtypes = [vp, ctypes.POINTER(DgfClassTime), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.dgf_measure_fma_peak.argtypes = [ctypes.c_int, _dp, _dp]
     lib.dgf_strerror.argtypes = [ctypes.c_int]
     lib.dgf_strerror.restype = ctypes.c_char_p
     lib.dgf_last_error.argtypes = []
@@ -112,3 +125,10 @@ def default_options(**kw) -> DgfOptions:
         if v is not None:
             setattr(o, k, v)
     return o
+
+
+def measure_fma_peak(device: int = 0):
+    """(FP64, FP32) FMA throughput in TFLOP/s measured on `device`."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    check(load().dgf_measure_fma_peak(int(device), ctypes.byref(a), ctypes.byref(b)), "dgf_measure_fma_peak")
+    return a.value, b.value

@@ -11,7 +11,7 @@
 #include <string>
 #include <vector>
 
-#include "dgf_internal.h"
+#include "dgf_ctx.h"
 #include "dgf_md.cuh"
 
 using namespace dgf;
@@ -171,38 +171,6 @@ void sph_table_host(std::vector<double> &out) {
 
 }  // namespace dgf
 
-// ----------------------------------------------------------------- context
-struct ClassPlan {
-  int X, Y;
-  int64_t off;        // offset of this class pair's qoff array in the plan buffer
-  int64_t nquartet;
-};
-
-struct dgf_ctx {
-  int device = 0, nbf = 0, natom = 0, nshell = 0, spherical = 1, maxl = 0, nsm = 148;
-  std::vector<double> xyz, charge;
-  std::vector<int> sh_l, sh_atom, sh_ao, sh_nprim, sh_p0;
-  std::vector<double> sh_a, sh_c;
-  std::vector<PairRec> pairs;  // class-major, Schwarz-descending inside a class
-  int cls_off[kNumPairClass + 1] = {0};
-  std::vector<PrimPair> pp;
-  PairRec *d_pairs = nullptr;
-  PrimPair *d_pp = nullptr;
-  double *d_boys = nullptr, *d_sph = nullptr;
-  // per-call buffers
-  int cap_slots = 0, cap_io = 0;
-  double *d_D = nullptr, *d_Ds = nullptr, *d_Fh = nullptr, *d_io = nullptr;
-  float *d_dmax = nullptr;
-  unsigned long long *d_cnt = nullptr;
-  // quartet plan, cached by Schwarz threshold
-  double plan_thrs = -1.0;
-  std::vector<ClassPlan> plan;
-  int64_t *d_qoff = nullptr;
-  size_t qoff_cap = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-};
-
 static void free_ctx(dgf_ctx *c) {
   if (!c) return;
   int prev = 0;
@@ -215,28 +183,135 @@ static void free_ctx(dgf_ctx *c) {
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   cudaSetDevice(prev);
   delete c;
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
 
-static int launch_class(dgf_ctx *c, int X, int Y, JKArgs &args, cudaStream_t st) {
-  const ClassKernel &k = jk_kernel(X, Y, 0);
-  int64_t grid64 = std::min<int64_t>(args.nquartet, (int64_t)c->nsm * 16);
+static int cls_l1(int X) { return (X == 0) ? 0 : (X <= 2) ? 1 : (X <= 5) ? 2 : 3; }
+
+static int launch_class(dgf_ctx *c, int X, int Y, JKArgs &args, cudaStream_t st, int precision) {
+  const ClassKernel &k = jk_kernel(X, Y, precision);
+  const bool thread_kernel = (k.smem == 0);
+  const int64_t per_block = thread_kernel ? k.block : 1;  // thread kernels: a quartet per thread
+  const int64_t nq = args.nquartet - args.q_begin;
+  if (nq <= 0 && !args.diag_out) return DGF_OK;
+  int64_t grid64 = std::min<int64_t>((nq + per_block - 1) / per_block, (int64_t)c->nsm * 16);
   int grid = (int)std::max<int64_t>(grid64, 1);
+  const bool prof = c->profiling && !args.diag_out;
+  if (prof) {
+    cudaEvent_t e0, e1;
+    DGF_CUDA_CHECK(cudaEventCreate(&e0));
+    DGF_CUDA_CHECK(cudaEventCreate(&e1));
+    c->prof_ev.push_back(e0);
+    c->prof_ev.push_back(e1);
+    DGF_CUDA_CHECK(cudaEventRecord(e0, st));
+  }
   k.launch(args, grid, k.block, k.smem, st);
   DGF_CUDA_CHECK(cudaGetLastError());
+  if (prof) {
+    DGF_CUDA_CHECK(cudaEventRecord(c->prof_ev.back(), st));
+    dgf_class_time r;
+    r.la = cls_l1(X);
+    r.lb = X - r.la * (r.la + 1) / 2;
+    r.lc = cls_l1(Y);
+    r.ld = Y - r.lc * (r.lc + 1) / 2;
+    r.precision = (precision == 1) ? 32 : 64;
+    r.kernel = thread_kernel ? 0 : 1;
+    r.quartets = args.nquartet - args.q_begin;
+    r.evaluated = 0;
+    r.prim_quartets = 0;
+    r.ms = 0.0;
+    c->prof.push_back(r);
+  }
   return DGF_OK;
+}
+
+static int finish_profile(dgf_ctx *c, cudaStream_t st) {
+  if (!c->profiling) return DGF_OK;
+  DGF_CUDA_CHECK(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < c->prof.size(); ++i) {
+    float ms = 0.f;
+    DGF_CUDA_CHECK(cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]));
+    c->prof[i].ms = ms;
+  }
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+  c->prof_ev.clear();
+  return DGF_OK;
+}
+
+extern "C" int dgf_set_profiling(dgf_ctx *c, int on) {
+  if (!c) DGF_FAIL(DGF_ERR_ARG, "ctx is NULL");
+  c->profiling = on ? 1 : 0;
+  return DGF_OK;
+}
+
+extern "C" int dgf_get_profile(const dgf_ctx *c, dgf_class_time *out, int max, int *count) {
+  if (!c || (max > 0 && !out)) DGF_FAIL(DGF_ERR_ARG, "NULL argument");
+  const int n = std::min<int>(max, (int)c->prof.size());
+  for (int i = 0; i < n; ++i) out[i] = c->prof[i];
+  if (count) *count = (int)c->prof.size();
+  return DGF_OK;
+}
+
+// Register-resident FMA chains: 8 independent accumulators per thread.
+template <typename T>
+__global__ void fma_peak_kernel(T *out, int iters, T a, T b) {
+  T x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      x0 = x0 * a + b; x1 = x1 * a + b; x2 = x2 * a + b; x3 = x3 * a + b;
+      x4 = x4 * a + b; x5 = x5 * a + b; x6 = x6 * a + b; x7 = x7 * a + b;
+    }
+  }
+  const T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == T(-1)) out[0] = s;  // keeps the chains live
+}
+
+template <typename T>
+static int fma_peak(int device, double *tflops) {
+  cudaDeviceProp prop;
+  DGF_CUDA_CHECK(cudaGetDeviceProperties(&prop, device));
+  T *d = nullptr;
+  DGF_CUDA_CHECK(cudaMalloc(&d, sizeof(T)));
+  const int block = 256, grid = prop.multiProcessorCount * 8, iters = 4096;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  fma_peak_kernel<T><<<grid, block>>>(d, 64, T(0.999999), T(1e-7));
+  float best = 1e30f;
+  for (int rep = 0; rep < 3; ++rep) {
+    cudaEventRecord(e0);
+    fma_peak_kernel<T><<<grid, block>>>(d, iters, T(0.999999), T(1e-7));
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    best = std::min(best, ms);
+  }
+  cudaError_t err = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  DGF_CUDA_CHECK(err);
+  const double flops = 2.0 * 8 * 16 * (double)iters * block * grid;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return DGF_OK;
+}
+
+extern "C" int dgf_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    DGF_FAIL(DGF_ERR_NODEVICE, "no such CUDA device");
+  }
+  DeviceGuard g(device);
+  int r = DGF_OK;
+  if (fp64_tflops) r = fma_peak<double>(device, fp64_tflops);
+  if (!r && fp32_tflops) r = fma_peak<float>(device, fp32_tflops);
+  return r;
 }
 
 static JKArgs base_args(dgf_ctx *c) {
@@ -267,7 +342,7 @@ static int compute_schwarz(dgf_ctx *c) {
     a.same_class = 1;
     a.boys = c->d_boys + (size_t)(2 * (la + (X - la * (la + 1) / 2))) * kBoysTableDoubles;
     a.diag_out = d_q + c->cls_off[X];
-    int st = launch_class(c, X, X, a, c->stream);
+    int st = launch_class(c, X, X, a, c->stream, 2);
     if (st) {
       cudaFree(d_q);
       return st;
@@ -288,6 +363,8 @@ extern "C" void dgf_default_options(dgf_options *opt) {
   opt->ifthrs = 20;
   opt->hfxfac = 1.0;
   opt->mixed_cutoff = 0.0;
+  opt->shard_index = 0;
+  opt->shard_count = 1;
 }
 
 extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
@@ -411,7 +488,7 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
   sph_table_host(sph);
   if (dev_alloc(&c->d_boys, boys.size()) != cudaSuccess || dev_alloc(&c->d_sph, sph.size()) != cudaSuccess ||
       dev_alloc(&c->d_pp, c->pp.size()) != cudaSuccess || dev_alloc(&c->d_pairs, c->pairs.size()) != cudaSuccess ||
-      dev_alloc(&c->d_cnt, 8) != cudaSuccess) {
+      dev_alloc(&c->d_cnt, 4 * kCounterSlots) != cudaSuccess) {
     cudaGetLastError();
     DGF_FAIL(DGF_ERR_NOMEM, "device allocation failed while creating the context");
   }
@@ -571,6 +648,8 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   dgf_default_options(&o);
   if (opt) o = *opt;
   if (!(o.thrs >= 0.0)) DGF_FAIL(DGF_ERR_ARG, "thrs must be >= 0");
+  if (o.shard_count <= 0) o.shard_count = 1;
+  if (o.shard_index < 0 || o.shard_index >= o.shard_count) DGF_FAIL(DGF_ERR_ARG, "shard_index out of range");
   const int N = c->nbf;
   const size_t n2 = (size_t)N * N;
   // Decode IFCTYP into density slots and output combinations.
@@ -613,11 +692,17 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   const int chunk = std::min(kMaxSlots, std::max(nslot_total, 1));
   st_code = ensure_slots(c, chunk);
   if (st_code) return st_code;
-  DGF_CUDA_CHECK(cudaMemsetAsync(c->d_cnt, 0, 8 * sizeof(unsigned long long), st));
+  if (c->profiling) {
+    for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+    c->prof_ev.clear();
+    c->prof.clear();
+  }
+  DGF_CUDA_CHECK(cudaMemsetAsync(c->d_cnt, 0, 4 * kCounterSlots * sizeof(unsigned long long), st));
   DGF_CUDA_CHECK(cudaEventRecord(c->ev0, st));
   const bool need_dmax = (o.ifthrs < 20) || (o.mixed_cutoff > 0.0);
-  int64_t launches = 0, total_q = 0;
-  for (const ClassPlan &cp : c->plan) total_q += cp.nquartet;
+  int64_t launches = 0, total_q = 0, nlaunch_class = 0;
+  for (const ClassPlan &cp : c->plan)
+    total_q += cp.nquartet * (o.shard_index + 1) / o.shard_count - cp.nquartet * o.shard_index / o.shard_count;
   const int eb = 256, eg = (int)std::min<size_t>((n2 + eb - 1) / eb, (size_t)c->nsm * 8);
   // Zero outputs that have no contributions.
   for (int k = 0; k < ndmat; ++k)
@@ -657,26 +742,32 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     a.dens_thr = (o.ifthrs < 20) ? std::pow(10.0, -(double)o.ifthrs) : 0.0;
     a.split = o.mixed_cutoff;
     a.mode = 0;
-    a.counters = c->d_cnt;
     for (const ClassPlan &cp : c->plan) {
       a.bra = c->d_pairs + c->cls_off[cp.X];
       a.ket = c->d_pairs + c->cls_off[cp.Y];
       a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
       a.same_class = (cp.X == cp.Y);
       a.qoff = c->d_qoff + cp.off;
-      a.nquartet = cp.nquartet;
+      a.q_begin = cp.nquartet * o.shard_index / o.shard_count;
+      a.nquartet = cp.nquartet * (o.shard_index + 1) / o.shard_count;
       // Boys table of order L = la+lb+lc+ld.
       const int la = (cp.X == 0) ? 0 : (cp.X <= 2) ? 1 : (cp.X <= 5) ? 2 : 3;
       const int lb = cp.X - la * (la + 1) / 2;
       const int lc = (cp.Y == 0) ? 0 : (cp.Y <= 2) ? 1 : (cp.Y <= 5) ? 2 : 3;
       const int ld = cp.Y - lc * (lc + 1) / 2;
       a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-      int r = launch_class(c, cp.X, cp.Y, a, st);
-      if (r) {
-        if (d_shinfo) cudaFree(d_shinfo);
-        return r;
+      const bool split = o.mixed_cutoff > 0.0 && jk_kernel(cp.X, cp.Y, 1).launch != nullptr;
+      for (int part = 0; part < (split ? 2 : 1); ++part) {
+        a.mode = split ? 1 + part : 0;
+        a.counters = c->d_cnt + 4 * (nlaunch_class % kCounterSlots);
+        ++nlaunch_class;
+        int r = launch_class(c, cp.X, cp.Y, a, st, split && part == 1 ? 1 : 0);
+        if (r) {
+          if (d_shinfo) cudaFree(d_shinfo);
+          return r;
+        }
+        ++launches;
       }
-      ++launches;
     }
     // Combine the slots of this chunk into the outputs they belong to.
     for (int k = 0; k < ndmat; ++k) {
@@ -689,19 +780,30 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   }
   DGF_CUDA_CHECK(cudaGetLastError());
   DGF_CUDA_CHECK(cudaEventRecord(c->ev1, st));
+  st_code = finish_profile(c, st);
+  if (st_code) return st_code;
   if (d_shinfo) {
     cudaStreamSynchronize(st);
     cudaFree(d_shinfo);
   }
-  if (stats) {
-    unsigned long long cnt[8];
-    DGF_CUDA_CHECK(cudaMemcpyAsync(cnt, c->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+  if (stats || c->profiling) {
+    std::vector<unsigned long long> all(4 * kCounterSlots);
+    DGF_CUDA_CHECK(cudaMemcpyAsync(all.data(), c->d_cnt, all.size() * 8, cudaMemcpyDeviceToHost, st));
     DGF_CUDA_CHECK(cudaStreamSynchronize(st));
+    unsigned long long cnt[4] = {0, 0, 0, 0};
+    for (int i = 0; i < kCounterSlots; ++i)
+      for (int k = 0; k < 4; ++k) cnt[k] += all[4 * i + k];
+    if (c->profiling)
+      for (size_t i = 0; i < c->prof.size() && i < (size_t)kCounterSlots; ++i) {
+        c->prof[i].evaluated = (int64_t)all[4 * i];
+        c->prof[i].prim_quartets = (int64_t)all[4 * i + 1];
+      }
+    if (!stats) return DGF_OK;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     stats->quartets_total = total_q;
-    stats->quartets_fp64 = (int64_t)cnt[0];
-    stats->quartets_fp32 = 0;
+    stats->quartets_fp64 = (int64_t)(cnt[0] - cnt[3]);
+    stats->quartets_fp32 = (int64_t)cnt[3];
     stats->quartets_skipped = (int64_t)cnt[2];
     stats->prim_quartets = (int64_t)cnt[1];
     stats->kernel_launches = launches;

@@ -57,7 +57,8 @@ struct JKArgs {
   const int64_t *qoff;      // prefix sums of ket partners per bra (nbra+1), device
   int nbra;
   int same_class;           // bra class == ket class (canonical ket <= bra)
-  int64_t nquartet;
+  int64_t q_begin;          // first quartet of this launch (shard start)
+  int64_t nquartet;         // one past the last quartet of this launch
   const PrimPair *pp;
   const double *boys;       // table for M = L of this class
   const double *sph;        // Cartesian->spherical tables, see sph_offset()

@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
   const int FC = nfun(LC, a.spherical), FD = nfun(LD, a.spherical);
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
 
-  for (int64_t q = blockIdx.x; q < a.nquartet; q += gridDim.x) {
+  for (int64_t q = a.q_begin + blockIdx.x; q < a.nquartet; q += gridDim.x) {
     __syncthreads();
     if (tid == 0) {
       int ib, ic;

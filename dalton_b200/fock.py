@@ -71,7 +71,7 @@ class FockBuilder:
     def _ifctyp(ifctyp, nd):
         return np.ascontiguousarray(np.broadcast_to(np.asarray(ifctyp, dtype=np.int64), (nd,)))
 
-    def herfck(self, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, mixed_cutoff=0.0) -> np.ndarray:
+    def herfck(self, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, mixed_cutoff=0.0, shard=(0, 1)) -> np.ndarray:
         """F = [Y&1] J[D] - [Y&2] hfxfac/2 K[D] for host matrices (N,N) or (ndmat,N,N)."""
         d = np.ascontiguousarray(dmat, dtype=np.float64)
         single = d.ndim == 2
@@ -83,7 +83,8 @@ class FockBuilder:
         ift = self._ifctyp(ifctyp, nd)
         f = np.empty_like(d)
         opt = _lib.default_options(thrs=float(thrs), ifthrs=int(ifthrs), hfxfac=float(hfxfac),
-                                   mixed_cutoff=float(mixed_cutoff))
+                                   mixed_cutoff=float(mixed_cutoff), shard_index=int(shard[0]),
+                                   shard_count=int(shard[1]))
         st = _lib.DgfStats()
         _lib.check(self._lib.dgf_fock(self._h, nd, ift.ctypes.data_as(ctypes.POINTER(_lib.dgf_int)), _dp(d), _dp(f),
                                       ctypes.byref(opt), ctypes.byref(st)), "dgf_fock")
@@ -91,7 +92,7 @@ class FockBuilder:
         return f[0] if single else f
 
     def herfck_device(self, dmat, fmat=None, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, mixed_cutoff=0.0,
-                      stream=None, stats=True):
+                      stream=None, stats=True, shard=(0, 1)):
         """Device form: ``dmat`` a CUDA float64 tensor (N,N) or (ndmat,N,N)."""
         import torch
 
@@ -103,7 +104,8 @@ class FockBuilder:
             fmat = torch.empty_like(d)
         ift = self._ifctyp(ifctyp, nd)
         opt = _lib.default_options(thrs=float(thrs), ifthrs=int(ifthrs), hfxfac=float(hfxfac),
-                                   mixed_cutoff=float(mixed_cutoff))
+                                   mixed_cutoff=float(mixed_cutoff), shard_index=int(shard[0]),
+                                   shard_count=int(shard[1]))
         if stream is None:
             stream = torch.cuda.current_stream(d.device).cuda_stream
         st = _lib.DgfStats()
@@ -114,6 +116,17 @@ class FockBuilder:
         if stats:
             self.last_stats = st.as_dict()
         return fmat
+
+    def set_profiling(self, on: bool = True):
+        _lib.check(self._lib.dgf_set_profiling(self._h, 1 if on else 0), "dgf_set_profiling")
+
+    def profile(self) -> list[dict]:
+        """Per-class launch records of the last profiled Fock build."""
+        n = ctypes.c_int()
+        _lib.check(self._lib.dgf_get_profile(self._h, None, 0, ctypes.byref(n)), "dgf_get_profile")
+        arr = (_lib.DgfClassTime * max(n.value, 1))()
+        _lib.check(self._lib.dgf_get_profile(self._h, arr, n.value, ctypes.byref(n)), "dgf_get_profile")
+        return [arr[i].as_dict() for i in range(n.value)]
 
     def oneint(self):
         n = self.nbf

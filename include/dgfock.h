@@ -95,9 +95,16 @@ typedef struct {
   dgf_int ifthrs;
   double hfxfac;
   double mixed_cutoff;
+  /* Shard of the quartet queue this call evaluates: every class's canonical
+   * quartet list is cut into shard_count equal contiguous ranges and range
+   * shard_index is evaluated, so each shard does 1/shard_count of every
+   * class; F is then the partial sum of that shard (sum the shards, e.g.
+   * with an NCCL all-reduce, for the full matrix).  0 and 1 = everything. */
+  dgf_int shard_index;
+  dgf_int shard_count;
 } dgf_options;
 
-/* Default options: thrs 1e-12, ifthrs 20, hfxfac 1, mixed_cutoff 0. */
+/* Default options: thrs 1e-12, ifthrs 20, hfxfac 1, mixed_cutoff 0, one shard. */
 void dgf_default_options(dgf_options *opt);
 
 /* Create a context on CUDA device `device`: copies the basis to the device,
@@ -136,6 +143,31 @@ int dgf_oneint(dgf_ctx *ctx, double *S, double *T, double *V);
 /* One-electron + nuclear-repulsion part of the RHF gradient:
  * sum D_pq dh_pq/dx - sum W_pq dS_pq/dx + dVnn/dx, grad(natom,3). */
 int dgf_grad1e(dgf_ctx *ctx, const double *dmat, const double *wmat, double *grad);
+
+/* Per-launch profile of the last Fock build (enabled by dgf_set_profiling):
+ * one record per quartet-class kernel launch, timed with CUDA events on the
+ * launching stream. */
+typedef struct {
+  int32_t la, lb, lc, ld;   /* angular momenta of the class (ab|cd) */
+  int32_t precision;        /* 64 = FP64, 32 = FP32 contraction */
+  int32_t kernel;           /* 0 = thread-per-quartet, 1 = cooperative team */
+  int64_t quartets;         /* quartets of the class in the plan */
+  int64_t evaluated;        /* quartets this launch evaluated */
+  int64_t prim_quartets;    /* primitive quartets this launch evaluated */
+  double ms;                /* device time of the launch */
+} dgf_class_time;
+
+/* Turn per-launch profiling of dgf_fock / dgf_fock_device on (1) or off (0).
+ * While on, each call synchronises its stream at the end. */
+int dgf_set_profiling(dgf_ctx *ctx, int on);
+
+/* Copy up to `max` records of the last profiled call; *count = records. */
+int dgf_get_profile(const dgf_ctx *ctx, dgf_class_time *out, int max, int *count);
+
+/* Measurement helper (not part of the HERFCK contract): FP64 and FP32 FMA
+ * throughput of device `device` in TFLOP/s from a register-resident FMA
+ * loop, the denominator of the FP64-pipe roofline. */
+int dgf_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
 /* Number of basis functions, atoms and segmented shells of a context. */
 int dgf_info(const dgf_ctx *ctx, dgf_int *nbf, dgf_int *natom, dgf_int *nshell);

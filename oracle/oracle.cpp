@@ -470,8 +470,22 @@ int orc_eri_full(const orc_basis *b, double *eri) {
 // HERFCK semantics through FCKD03-style digestion of unique integrals
 // (DALTON/sirius/sirfck.F:1496-1547; IFCTYP decoding sirfck.F:45-57 and
 // DALTON/abacus/herfckcon.F:20-220).
+static int fock_core(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
+                     double hfxfac, double thrs, int stride, int offset, int64_t *nquartet);
+
 int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
              double hfxfac, double thrs) {
+  return fock_core(b, ndmat, ifctyp, dmat, fmat, hfxfac, thrs, 1, 0, nullptr);
+}
+
+int orc_fock_sampled(const orc_basis *b, const double *dmat, double *fmat, double thrs, int stride, int offset,
+                     int64_t *nquartet) {
+  const int64_t ift = 13;
+  return fock_core(b, 1, &ift, dmat, fmat, 1.0, thrs, stride, offset, nquartet);
+}
+
+static int fock_core(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
+                     double hfxfac, double thrs, int stride, int offset, int64_t *nquartet) {
   set_threads();
   Basis B = make_basis(b);
   int ns = (int)B.sh.size();
@@ -497,18 +511,21 @@ int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double 
   int npair = (int)pairs.size();
   std::vector<double> F(ndmat * N2, 0.0);
   double efac = 0.5 * hfxfac;
-#pragma omp parallel
+  int64_t nq_total = 0;
+#pragma omp parallel reduction(+ : nq_total)
   {
     std::vector<double> Fl(ndmat * N2, 0.0);
     EriWork w;
     std::vector<double> g, cart, tmp;
 #pragma omp for schedule(dynamic)
     for (int ab = npair - 1; ab >= 0; --ab) {
+      if (ab % stride != offset) continue;
       int sA = pairs[ab].first, sB = pairs[ab].second;
       double qab = Q[(size_t)sA * ns + sB];
       for (int cd = 0; cd <= ab; ++cd) {
         int sC = pairs[cd].first, sD = pairs[cd].second;
         if (qab * Q[(size_t)sC * ns + sD] < thrs) continue;
+        ++nq_total;
         shell_eri(B, sA, sB, sC, sD, g, w, cart, tmp);
         const Shell &A = B.sh[sA], &Bs = B.sh[sB], &C = B.sh[sC], &Dd = B.sh[sD];
         for (int i = 0; i < A.nf; ++i) {
@@ -559,6 +576,7 @@ int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double 
     for (size_t i = 0; i < F.size(); ++i) F[i] += Fl[i];
   }
   std::memcpy(fmat, F.data(), F.size() * sizeof(double));
+  if (nquartet) *nquartet = nq_total;
   return 0;
 }
 

@@ -61,6 +61,11 @@ int orc_schwarz(const orc_basis *b, double *q /* nshell^2 */, int64_t *shell_l, 
 int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat,
              double *fmat, double hfxfac, double thrs);
 
+/* Sampled J+K build (IFCTYP 13, hfxfac 1) over the bra pairs ab with
+ * ab % stride == offset, for CPU-baseline timing; *nquartet = quartets done. */
+int orc_fock_sampled(const orc_basis *b, const double *dmat, double *fmat, double thrs, int stride, int offset,
+                     int64_t *nquartet);
+
 /* Two-electron part of the RHF gradient: 1/2 sum (pq|rs)^x [D_pq D_rs - hfx/2 D_pr D_qs],
  * D the total (symmetric) density; grad (natom, 3) overwritten. */
 int orc_grad2e(const orc_basis *b, const double *dmat, double hfxfac, double thrs, double *grad);

@@ -51,6 +51,8 @@ def lib():
         _lib.orc_sph_matrix.argtypes = [ctypes.c_int, _dp]
         _lib.orc_set_threads.argtypes = [ctypes.c_int]
         _lib.orc_nshell.argtypes = [ctypes.POINTER(OrcBasis)]
+        _lib.orc_fock_sampled.argtypes = [ctypes.POINTER(OrcBasis), _dp, _dp, ctypes.c_double, ctypes.c_int,
+                                          ctypes.c_int, _i64p]
         _lib.orc_schwarz.argtypes = [ctypes.POINTER(OrcBasis), _dp, _i64p, _i64p, _i64p]
     return _lib
 
@@ -145,6 +147,17 @@ def fock(bs, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12) -> np.ndarray:
     lib().orc_fock(ctypes.byref(h.s), nd, _p(ift, ctypes.c_int64), _p(d, ctypes.c_double),
                    _p(f, ctypes.c_double), float(hfxfac), float(thrs))
     return f[0] if single else f
+
+
+def fock_sampled(bs, dmat, stride, offset=0, thrs=1e-12):
+    """J+K over every stride-th bra pair; returns (partial F, quartets done)."""
+    h = _Holder(bs)
+    d = np.ascontiguousarray(dmat, dtype=np.float64)
+    f = np.zeros_like(d)
+    nq = ctypes.c_int64()
+    lib().orc_fock_sampled(ctypes.byref(h.s), _p(d, ctypes.c_double), _p(f, ctypes.c_double), float(thrs),
+                           int(stride), int(offset), ctypes.byref(nq))
+    return f, nq.value
 
 
 def grad2e(bs, dmat, hfxfac=1.0, thrs=1e-12) -> np.ndarray:
