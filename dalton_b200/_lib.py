@@ -19,7 +19,7 @@ DGF_OK, DGF_ERR_ARG, DGF_ERR_NOMEM, DGF_ERR_CUDA, DGF_ERR_UNSUPPORTED, DGF_ERR_T
 
 # Every symbol include/dgfock.h declares.
 EXPORTS = ["dgf_default_options", "dgf_create", "dgf_destroy", "dgf_fock", "dgf_fock_device", "dgf_grad2e",
-           "dgf_grad2e_device", "dgf_oneint", "dgf_grad1e", "dgf_set_profiling", "dgf_get_profile",
+           "dgf_grad2e_device", "dgf_grad2e_bilinear_device", "dgf_oneint", "dgf_grad1e", "dgf_set_profiling", "dgf_get_profile",
            "dgf_measure_fma_peak", "dgf_info", "dgf_strerror", "dgf_last_error"]
 
 
@@ -82,6 +82,7 @@ def load() -> ctypes.CDLL:
                                     ctypes.POINTER(DgfStats)]
     lib.dgf_grad2e.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, _dp]
     lib.dgf_grad2e_device.argtypes = [vp, vp, ctypes.c_double, ctypes.c_double, vp, vp]
+    lib.dgf_grad2e_bilinear_device.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_double, vp, vp]
     lib.dgf_oneint.argtypes = [vp, _dp, _dp, _dp]
     lib.dgf_grad1e.argtypes = [vp, _dp, _dp, _dp]
     lib.dgf_info.argtypes = [vp, _ip, _ip, _ip]

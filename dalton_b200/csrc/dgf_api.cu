@@ -465,7 +465,7 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
           q.PBy = q.Py - xb[1];
           q.PBz = q.Pz - xb[2];
           q.K = c->sh_c[c->sh_p0[sa] + i] * c->sh_c[c->sh_p0[sb] + j] * std::exp(-mu * ab2) * r2pi52 / p;
-          q.pad = 0.0;
+          q.ea = ea;
           pp.push_back(q);
         }
       r.npp = (int)pp.size() - r.pp0;
@@ -570,6 +570,8 @@ static int build_plan(dgf_ctx *c, double thrs) {
   c->plan_thrs = thrs;
   return DGF_OK;
 }
+
+int dgf_plan_for(dgf_ctx *c, double thrs) { return build_plan(c, thrs); }
 
 static int ensure_slots(dgf_ctx *c, int nslot) {
   if (nslot <= c->cap_slots) return DGF_OK;

@@ -409,12 +409,3 @@ extern "C" int dgf_grad1e(dgf_ctx *c, const double *dmat, const double *wmat, do
   memcpy(grad, gr.data(), gr.size() * 8);
   return DGF_OK;
 }
-
-extern "C" int dgf_grad2e(dgf_ctx *, const double *, double, double, double *) {
-  dgf::set_error(__FILE__, __LINE__, "two-electron gradient not built yet");
-  return DGF_ERR_UNSUPPORTED;
-}
-extern "C" int dgf_grad2e_device(dgf_ctx *, const double *, double, double, double *, void *) {
-  dgf::set_error(__FILE__, __LINE__, "two-electron gradient not built yet");
-  return DGF_ERR_UNSUPPORTED;
-}

@@ -36,7 +36,7 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // K = c_a c_b exp(-mu |AB|^2) sqrt(2 pi^(5/2)) / p, Dalton's FAC12 with R2PI52
 // (DALTON/abacus/her2odc.F:229-231, DALTON/include/pi.h:9-14).
 struct PrimPair {
-  double p, Px, Py, Pz, PAx, PAy, PAz, PBx, PBy, PBz, K, pad;
+  double p, Px, Py, Pz, PAx, PAy, PAz, PBx, PBy, PBz, K, ea;  // ea: exponent of A (B's is p - ea)
 };
 
 // Shell pair record in a class list (sorted by Schwarz factor, descending).
@@ -78,6 +78,10 @@ struct JKArgs {
   int mode;                 // 0: all, 1: bound >= split only, 2: bound < split only
   double *diag_out;         // Schwarz mode: sqrt(max |(ab|ab)|) per bra pair, no digestion
   unsigned long long *counters;  // [0] quartets done, [1] primitive quartets, [2] skipped
+  // gradient mode (dgf_grad2e): densities D1, D2 (N*N) and grad (natom*3)
+  const double *G1, *G2;
+  double *grad;
+  double hfx;
 };
 
 // Offset of the l-block of the Cartesian->spherical table: rows m=-l..l,

@@ -136,6 +136,16 @@ int dgf_grad2e(dgf_ctx *ctx, const double *dmat, double hfxfac, double thrs, dou
 int dgf_grad2e_device(dgf_ctx *ctx, const double *dmat_device, double hfxfac, double thrs, double *grad_device,
                       void *stream);
 
+/* Bilinear form of the two-electron gradient, device pointers: grad = sum
+ * over canonical quartets of d(ab|cd)/dx times the symmetrised product
+ * 2 (D1_ab D2_cd + D2_ab D1_cd) - hfxfac/2 (D1_ac D2_bd + D2_ac D1_bd +
+ * D1_ad D2_bc + D2_ad D1_bc) (weighted for coinciding shells).  With
+ * D1 = D2 = D it equals dgf_grad2e; with D1 = C a symmetric cotangent of
+ * G = F(D) it is half of d<C, G(D)>/dx (the backward pass of the build).
+ * No counterpart in Dalton, which only forms the D1 = D2 case (INTEX1). */
+int dgf_grad2e_bilinear_device(dgf_ctx *ctx, const double *d1_device, const double *d2_device, double hfxfac,
+                               double thrs, double *grad_device, void *stream);
+
 /* One-electron integrals S, T, V (N x N each, host pointers, any may be
  * NULL): the HER1 integrals the SCF host needs next to the Fock build. */
 int dgf_oneint(dgf_ctx *ctx, double *S, double *T, double *V);
