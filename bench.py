@@ -258,6 +258,10 @@ def main():
     scf_s = time.perf_counter() - t0
     D = scf64["dmat"].contiguous()
     H = scf64["H"]
+    # Per-class kernel choice on this density (FP64 and FP32 candidates).
+    t0 = time.perf_counter()
+    tuning = fb.autotune(D, thrs=THRS)
+    tune_s = time.perf_counter() - t0
     enuc = scf64["enuc"]
     # Accuracy of the mixed build at the converged density.
     F64 = build(D, False).clone()
@@ -387,6 +391,7 @@ def main():
             "e2e": {"value": quartets / (e2e_ms * 1e-3), "unit": "quartets/s", "ms": e2e_ms,
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
             "roofline": roofline, "build_tflops_model": build_tflops,
+            "autotune": {"seconds": tune_s, "candidates_timed": len(tuning)},
             "peaks_measured": {"fp64_tflops": fp64_peak, "fp32_tflops": fp32_peak},
             "gpu_launches": int((lmx if headline_mixed else l64)),
             "clocks": clk, "cpu_baseline": cpu,

@@ -20,7 +20,7 @@ DGF_OK, DGF_ERR_ARG, DGF_ERR_NOMEM, DGF_ERR_CUDA, DGF_ERR_UNSUPPORTED, DGF_ERR_T
 # Every symbol include/dgfock.h declares.
 EXPORTS = ["dgf_default_options", "dgf_create", "dgf_destroy", "dgf_fock", "dgf_fock_device", "dgf_grad2e",
            "dgf_grad2e_device", "dgf_grad2e_bilinear_device", "dgf_oneint", "dgf_grad1e", "dgf_set_profiling", "dgf_get_profile",
-           "dgf_measure_fma_peak", "dgf_info", "dgf_strerror", "dgf_last_error"]
+           "dgf_measure_fma_peak", "dgf_autotune", "dgf_info", "dgf_strerror", "dgf_last_error"]
 
 
 class DgfBasis(ctypes.Structure):
@@ -89,6 +89,7 @@ def load() -> ctypes.CDLL:
     lib.dgf_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dgf_get_profile.argtypes = [vp, ctypes.POINTER(DgfClassTime), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.dgf_measure_fma_peak.argtypes = [ctypes.c_int, _dp, _dp]
+    lib.dgf_autotune.argtypes = [vp, vp, ctypes.POINTER(DgfOptions), vp, ctypes.c_char_p, ctypes.c_size_t]
     lib.dgf_strerror.argtypes = [ctypes.c_int]
     lib.dgf_strerror.restype = ctypes.c_char_p
     lib.dgf_last_error.argtypes = []

@@ -9,6 +9,7 @@ from __future__ import annotations
 import concurrent.futures as cf
 import glob
 import os
+import re
 import subprocess
 import sys
 
@@ -24,9 +25,22 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
          "-ccbin", "g++", "-I", INCLUDE, "-I", CSRC]
 
 
-def _headers():
-    return glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
-        glob.glob(os.path.join(INCLUDE, "*.h"))
+def _deps(path, seen=None):
+    """Local headers a source includes, recursively (#include "...")."""
+    seen = set() if seen is None else seen
+    with open(path) as f:
+        for line in f:
+            m = re.match(r'\s*#\s*include\s+"([^"]+)"', line)
+            if not m:
+                continue
+            for base in (os.path.dirname(path), CSRC, INCLUDE):
+                cand = os.path.normpath(os.path.join(base, m.group(1)))
+                if os.path.exists(cand):
+                    if cand not in seen:
+                        seen.add(cand)
+                        _deps(cand, seen)
+                    break
+    return seen
 
 
 def _stale(target, deps):
@@ -38,7 +52,7 @@ def _stale(target, deps):
 
 def _compile(src, extra):
     obj = os.path.join(BUILD, os.path.basename(src).replace(".cu", ".o"))
-    if not _stale(obj, [src] + _headers()):
+    if not _stale(obj, [src] + sorted(_deps(src))):
         return obj, ""
     cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -191,8 +191,27 @@ static void free_ctx(dgf_ctx *c) {
 
 static int cls_l1(int X) { return (X == 0) ? 0 : (X <= 2) ? 1 : (X <= 5) ? 2 : 3; }
 
+// Kernel for class pair (X, Y): precision 0 = FP64 (the context's choice),
+// 1 = FP32 thread kernel, 2 = FP64 team kernel (Schwarz pre-pass).
+static const ClassKernel &select_kernel(const dgf_ctx *c, int X, int Y, int precision) {
+  if (precision == 2) return jk_kernel(X, Y, 2);
+  const int p = precision ? 1 : 0;
+  const int v = c->choice[X][Y][p];
+  const ClassKernel &k = jk_kernel_variant(X, Y, p, v);
+  if (k.launch) return k;
+  return jk_kernel(X, Y, precision);
+}
+
+static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs &args, cudaStream_t st,
+                         int precision);
+
 static int launch_class(dgf_ctx *c, int X, int Y, JKArgs &args, cudaStream_t st, int precision) {
-  const ClassKernel &k = jk_kernel(X, Y, precision);
+  return launch_kernel(c, select_kernel(c, X, Y, precision), X, Y, args, st, precision);
+}
+
+static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs &args, cudaStream_t st,
+                         int precision) {
+  if (!k.launch) DGF_FAIL(DGF_ERR_UNSUPPORTED, "no kernel for this class and precision");
   const bool thread_kernel = (k.smem == 0);
   const int64_t per_block = thread_kernel ? k.block : 1;  // thread kernels: a quartet per thread
   const int64_t nq = args.nquartet - args.q_begin;
@@ -219,6 +238,7 @@ static int launch_class(dgf_ctx *c, int X, int Y, JKArgs &args, cudaStream_t st,
     r.ld = Y - r.lc * (r.lc + 1) / 2;
     r.precision = (precision == 1) ? 32 : 64;
     r.kernel = thread_kernel ? 0 : 1;
+    (void)k;
     r.quartets = args.nquartet - args.q_begin;
     r.evaluated = 0;
     r.prim_quartets = 0;
@@ -868,3 +888,83 @@ extern "C" const char *dgf_strerror(int s) {
 }
 
 extern "C" const char *dgf_last_error(void) { return dgf::g_last_error.c_str(); }
+
+// Per-class autotuner: times every candidate kernel of every class pair of
+// the current plan on the given density (team kernel and each thread-kernel
+// chunk variant, FP64 and FP32) with CUDA events and keeps the fastest.
+extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_options *opt, void *stream,
+                            char *report, size_t report_len) {
+  if (!c || !dmat_device) DGF_FAIL(DGF_ERR_ARG, "NULL argument");
+  DeviceGuard g(c->device);
+  dgf_options o;
+  dgf_default_options(&o);
+  if (opt) o = *opt;
+  cudaStream_t st = (cudaStream_t)stream;
+  int r = build_plan(c, o.thrs);
+  if (r) return r;
+  r = ensure_slots(c, 1);
+  if (r) return r;
+  const size_t n2 = (size_t)c->nbf * c->nbf;
+  const int eb = 256, eg = (int)std::min<size_t>((n2 + eb - 1) / eb, (size_t)c->nsm * 8);
+  prep_slot_kernel<<<eg, eb, 0, st>>>(dmat_device, c->d_D, c->d_Ds, c->nbf, 2);
+  DGF_CUDA_CHECK(cudaGetLastError());
+  cudaEvent_t e0, e1;
+  DGF_CUDA_CHECK(cudaEventCreate(&e0));
+  DGF_CUDA_CHECK(cudaEventCreate(&e1));
+  std::string rep = "[";
+  const int saved_prof = c->profiling;
+  c->profiling = 0;
+  for (const ClassPlan &cp : c->plan) {
+    JKArgs a = base_args(c);
+    a.nslot = 1;
+    a.D = c->d_D;
+    a.Ds = c->d_Ds;
+    a.Fh = c->d_Fh;
+    a.jscale[0] = 1.0;
+    a.kscale[0] = 0.5 * o.hfxfac;
+    a.bra = c->d_pairs + c->cls_off[cp.X];
+    a.ket = c->d_pairs + c->cls_off[cp.Y];
+    a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
+    a.same_class = (cp.X == cp.Y);
+    a.qoff = c->d_qoff + cp.off;
+    a.q_begin = 0;
+    a.nquartet = cp.nquartet;
+    const int la = cls_l1(cp.X), lb = cp.X - la * (la + 1) / 2, lc = cls_l1(cp.Y), ld = cp.Y - lc * (lc + 1) / 2;
+    a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
+    for (int p = 0; p < 2; ++p) {
+      float best = 1e30f;
+      int bestv = c->choice[cp.X][cp.Y][p];
+      for (int v = -1; v < kThreadVariants; ++v) {
+        const ClassKernel &k = jk_kernel_variant(cp.X, cp.Y, p, v);
+        if (!k.launch) continue;
+        float ms = 0.f;
+        for (int rep2 = 0; rep2 < 2; ++rep2) {  // first launch warms caches
+          DGF_CUDA_CHECK(cudaEventRecord(e0, st));
+          r = launch_kernel(c, k, cp.X, cp.Y, a, st, p);
+          if (r) return r;
+          DGF_CUDA_CHECK(cudaEventRecord(e1, st));
+          DGF_CUDA_CHECK(cudaEventSynchronize(e1));
+          DGF_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        }
+        char buf[160];
+        snprintf(buf, sizeof(buf), "%s{\"class\":[%d,%d,%d,%d],\"precision\":%d,\"variant\":%d,\"chunks\":%d,\"ms\":%.4f}",
+                 rep.size() > 1 ? "," : "", la, lb, lc, ld, p ? 32 : 64, v, k.chunks, ms);
+        rep += buf;
+        if (ms < best) {
+          best = ms;
+          bestv = v;
+        }
+      }
+      c->choice[cp.X][cp.Y][p] = bestv;
+    }
+  }
+  c->profiling = saved_prof;
+  rep += "]";
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (report && report_len) {
+    strncpy(report, rep.c_str(), report_len - 1);
+    report[report_len - 1] = 0;
+  }
+  return DGF_OK;
+}

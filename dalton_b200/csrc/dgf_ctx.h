@@ -35,6 +35,9 @@ struct dgf_ctx {
   size_t qoff_cap = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // kernel choice per class pair and precision (-1 = team kernel, >= 0 =
+  // thread-kernel variant), set by the autotuner; 0 by default
+  int choice[dgf::kNumPairClass][dgf::kNumPairClass][2] = {};
   // per-class launch profiling (dgf_set_profiling)
   int profiling = 0;
   std::vector<cudaEvent_t> prof_ev;

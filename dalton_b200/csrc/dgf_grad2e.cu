@@ -20,7 +20,7 @@
 #include <vector>
 
 #include "dgf_ctx.h"
-#include "dgf_jk_thread.cuh"
+#include "dgf_md.cuh"
 
 using namespace dgf;
 

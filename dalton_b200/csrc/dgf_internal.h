@@ -98,11 +98,17 @@ typedef void (*JKLauncher)(const JKArgs &, int grid, int block, size_t smem, cud
 struct ClassKernel {
   JKLauncher launch;
   int block;
-  size_t smem;
+  size_t smem;   // dynamic shared memory (team kernels); 0 for thread kernels
+  int chunks;    // thread kernels: A-component chunks (grid.y)
 };
 
+constexpr int kThreadVariants = 2;
+
 // Per-class launch table (filled by dgf_jk.cu): index [X][Y] of pair classes.
+// precision: 0 = default FP64 kernel, 1 = FP32 thread kernel, 2 = team kernel.
 const ClassKernel &jk_kernel(int X, int Y, int precision);
+// variant -1 = team kernel, >= 0 = thread-kernel variant (precision 0/1).
+const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant);
 cudaError_t jk_prepare_all();
 
 void boys_table_host(std::vector<double> &out);       // [kBoysMaxM+1][kBoysTableDoubles]

@@ -1,0 +1,96 @@
+// Instantiation helpers of the quartet-class kernel table: each
+// dgf_jk_row<X>.cu fills row X (bra class X) of the table, so the rows
+// compile in parallel.
+#pragma once
+
+#include <utility>
+
+#include "dgf_jk_thread.cuh"
+
+namespace dgf {
+
+struct JKEntry {
+  ClassKernel team;
+  ClassKernel thr[2][kThreadVariants];  // [precision 0 = FP64, 1 = FP32][variant]
+  cudaError_t (*prepare)();
+};
+
+extern JKEntry g_jk_table[kNumPairClass][kNumPairClass];
+
+namespace jkinst {
+
+constexpr int cls_la(int X) { return X == 0 ? 0 : X <= 2 ? 1 : X <= 5 ? 2 : 3; }
+constexpr int cls_lb(int X) { return X - cls_la(X) * (cls_la(X) + 1) / 2; }
+
+constexpr bool thread_eligible(int LA, int LB, int LC, int LD) {
+  const int L = LA + LB + LC + LD;
+  if (LA == 3) return LB == 0 && LC == 0 && LD == 0;  // (fs|ss)
+  return L <= 5;
+}
+
+constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+constexpr int cmin(int a, int b) { return a < b ? a : b; }
+// A-chunk count keeping at most `target` accumulators per thread.
+constexpr int chunks_for(int LA, int LB, int LC, int LD, int target) {
+  return cmin(ncart(LA), cdiv(ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD), target));
+}
+
+template <int LA, int LB, int LC, int LD>
+void launch_team(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
+  jk_team_kernel<LA, LB, LC, LD><<<grid, block, smem, s>>>(a);
+}
+
+template <int LA, int LB, int LC, int LD, typename T, int CA>
+void launch_thread(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
+  jk_thread_kernel<LA, LB, LC, LD, T, CA><<<dim3(grid, CA), block, smem, s>>>(a);
+}
+
+template <int LA, int LB, int LC, int LD>
+cudaError_t prepare_team() {
+  return cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)TeamShape<LA, LB, LC, LD>::smem());
+}
+
+template <int LA, int LB, int LC, int LD, typename T, int CA>
+ClassKernel thread_entry() {
+  return ClassKernel{&launch_thread<LA, LB, LC, LD, T, CA>, kThreadBlock, 0, CA};
+}
+
+template <int X, int Y>
+void fill_one() {
+  constexpr int LA = cls_la(X), LB = cls_lb(X), LC = cls_la(Y), LD = cls_lb(Y);
+  using S = TeamShape<LA, LB, LC, LD>;
+  constexpr int work = S::NAB * S::NCD;
+  constexpr int block = work >= 512 ? 128 : work >= 64 ? 64 : 32;
+  JKEntry &e = g_jk_table[X][Y];
+  e.team = ClassKernel{&launch_team<LA, LB, LC, LD>, block, S::smem(), 1};
+  e.prepare = &prepare_team<LA, LB, LC, LD>;
+  for (int p = 0; p < 2; ++p)
+    for (int v = 0; v < kThreadVariants; ++v) e.thr[p][v] = ClassKernel{nullptr, 0, 0, 0};
+  if constexpr (thread_eligible(LA, LB, LC, LD)) {
+    constexpr int c64 = chunks_for(LA, LB, LC, LD, 27), c64b = cmin(ncart(LA), 2 * c64);
+    constexpr int c32 = chunks_for(LA, LB, LC, LD, 54), c32b = cmin(ncart(LA), 2 * c32);
+    e.thr[0][0] = thread_entry<LA, LB, LC, LD, double, c64>();
+    e.thr[1][0] = thread_entry<LA, LB, LC, LD, float, c32>();
+    if constexpr (c64b != c64) e.thr[0][1] = thread_entry<LA, LB, LC, LD, double, c64b>();
+    if constexpr (c32b != c32) e.thr[1][1] = thread_entry<LA, LB, LC, LD, float, c32b>();
+  }
+}
+
+template <int X, int... Ys>
+void fill_row(std::integer_sequence<int, Ys...>) {
+  (fill_one<X, Ys>(), ...);
+}
+
+}  // namespace jkinst
+}  // namespace dgf
+
+// Defines the static initialiser that fills row X of the table.
+#define DGF_JK_ROW(X)                                                                         \
+  namespace dgf {                                                                             \
+  namespace {                                                                                 \
+  struct RowInit##X {                                                                         \
+    RowInit##X() { jkinst::fill_row<X>(std::make_integer_sequence<int, X + 1>{}); }         \
+  } g_row_init_##X;                                                                           \
+  }                                                                                           \
+  }

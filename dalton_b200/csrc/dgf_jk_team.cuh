@@ -15,19 +15,6 @@
 
 namespace dgf {
 
-// Maps a flattened quartet index to (bra, ket) through the prefix array.
-__device__ __forceinline__ int find_bra(const int64_t *__restrict__ qoff, int nbra, int64_t q) {
-  int lo = 0, hi = nbra;
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (qoff[mid] <= q)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
 // Quartet bound Q_AB Q_CD max(4 max(|D|_AB,|D|_CD), |D|_AC,|D|_AD,|D|_BC,|D|_BD)
 // (SYMLOP, DALTON/abacus/her2drv.F:2666-2692).
 __device__ __forceinline__ double quartet_bound(const JKArgs &a, const PairRec &b, const PairRec &k) {

@@ -1,81 +1,159 @@
-// Register-resident McMurchie-Davidson J/K quartet kernel for the low
-// angular-momentum classes: one thread per contracted shell quartet, a warp
-// on 32 consecutive quartets of the class-sorted queue (mostly one bra pair
-// against 32 ket pairs, so bra data and the bra-side Coulomb block are
-// shared across the warp).
+// Register-resident McMurchie-Davidson J/K quartet kernel: one thread per
+// contracted shell quartet (optionally per chunk of its A-shell Cartesian
+// components), a warp on 32 consecutive quartets of the class-sorted queue.
+//
+// Consecutive quartets of the queue share their bra pair, so the bra
+// Hermite tables of the current bra primitive are built once per warp in
+// shared memory and read by broadcast; Boys function, R_tuv, the ket tables,
+// the ket transform and the accumulators stay in registers.  Warps whose
+// lanes hold different bra pairs process one bra group after another.
+//
+// CA splits the A shell's Cartesian components into CA compile-time chunks
+// (blockIdx.y); each chunk digests its partial spherical block (digestion is
+// linear in the integrals), which bounds the accumulator count per thread.
 //
 // Tc is the arithmetic type of the Hermite recursion and the Hermite ->
-// Cartesian contraction (double for the FP64 drop-in, float for the FP32 half
-// of the mixed form).  The Boys function, the prefactor and the digestion
-// (FP64 atomics into the half Fock matrices) are always FP64.
+// Cartesian contraction (double: FP64 drop-in; float: FP32 half of the mixed
+// form).  Boys function, prefactor and digestion (FP64 atomics into the half
+// Fock matrices) are FP64 in both.
 #pragma once
 
 #include "dgf_jk_team.cuh"
 
 namespace dgf {
 
-// R_tuv for t+u+v <= L in place (compact index), from Fs[n] = pref (-2a)^n F_n:
-// level by level from n = L-1 down to 0, each level in decreasing t+u+v so
-// the level-(n+1) values it reads are still in place.
-template <int L, typename T>
-__device__ __forceinline__ void hermite_r_inplace(const T *Fs, T x, T y, T z, T *R) {
-  R[0] = Fs[L];
+// Digestion of one quartet block g[FA][FB][FC][FD] (FA rows of A starting at
+// function a_off): J_ab (warp-reduced when the warp shares its bra pair),
+// J_cd, K_ac, K_ad, K_bc, K_bd as FP64 atomics into the half Fock matrices.
+template <int FA, int FB, int FC, int FD>
+__device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool work, bool uniform, int ib, int ic,
+                                          int ib0, const PairRec &kt, int a_off) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int N = a.nbf;
+  double w = 0.0;
+  PairRec br;
+  if (work) {
+    br = a.bra[ib];
+    w = 1.0;
+    if (br.same) w *= 0.5;
+    if (kt.same) w *= 0.5;
+    if (a.same_class && ib == ic) w *= 0.5;
+  }
+  const PairRec brw = a.bra[ib0];
+  for (int k = 0; k < a.nslot; ++k) {
+    const double *Dk = a.D + (size_t)k * N * N;
+    const double *Dsk = a.Ds + (size_t)k * N * N;
+    double *Fk = a.Fh + (size_t)k * N * N;
+    const double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
+    if (a.jscale[k] != 0.0) {
 #pragma unroll
-  for (int n = L - 1; n >= 0; --n) {
+      for (int x = 0; x < FA; ++x)
 #pragma unroll
-    for (int s = L - n; s >= 1; --s) {
+        for (int y = 0; y < FB; ++y) {
+          double s = 0.0;
+          if (work) {
 #pragma unroll
-      for (int w = 0; w <= s; ++w) {
+            for (int c = 0; c < FC; ++c)
 #pragma unroll
-        for (int v = 0; v <= w; ++v) {
-          const int u = w - v, t = s - w;
-          T val;
-          if (t > 0) {
-            val = x * R[tuv_index(t - 1, u, v)];
-            if (t > 1) val += T(t - 1) * R[tuv_index(t - 2, u, v)];
-          } else if (u > 0) {
-            val = y * R[tuv_index(t, u - 1, v)];
-            if (u > 1) val += T(u - 1) * R[tuv_index(t, u - 2, v)];
-          } else {
-            val = z * R[tuv_index(t, u, v - 1)];
-            if (v > 1) val += T(v - 1) * R[tuv_index(t, u, v - 2)];
+              for (int d = 0; d < FD; ++d)
+                s += g[((x * FB + y) * FC + c) * FD + d] * Dsk[(size_t)(kt.aoA + c) * N + kt.aoB + d];
+            s *= js;
           }
-          R[tuv_index(t, u, v)] = val;
+          if (uniform) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(full, s, off);
+            if (lane == 0) atomicAdd(Fk + (size_t)(brw.aoA + a_off + x) * N + brw.aoB + y, s);
+          } else if (work) {
+            atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + br.aoB + y, s);
+          }
+        }
+      if (work) {
+#pragma unroll
+        for (int c = 0; c < FC; ++c)
+#pragma unroll
+          for (int d = 0; d < FD; ++d) {
+            double s = 0.0;
+#pragma unroll
+            for (int x = 0; x < FA; ++x)
+#pragma unroll
+              for (int y = 0; y < FB; ++y)
+                s += g[((x * FB + y) * FC + c) * FD + d] * Dsk[(size_t)(br.aoA + a_off + x) * N + br.aoB + y];
+            atomicAdd(Fk + (size_t)(kt.aoA + c) * N + kt.aoB + d, js * s);
+          }
+      }
+    }
+    if (work && a.kscale[k] != 0.0) {
+#pragma unroll
+      for (int x = 0; x < FA; ++x) {
+#pragma unroll
+        for (int c = 0; c < FC; ++c) {
+          double s = 0.0;
+#pragma unroll
+          for (int y = 0; y < FB; ++y)
+#pragma unroll
+            for (int d = 0; d < FD; ++d)
+              s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoB + y) * N + kt.aoB + d];
+          atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, ks * s);
+        }
+#pragma unroll
+        for (int d = 0; d < FD; ++d) {
+          double s = 0.0;
+#pragma unroll
+          for (int y = 0; y < FB; ++y)
+#pragma unroll
+            for (int c = 0; c < FC; ++c)
+              s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoB + y) * N + kt.aoA + c];
+          atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoB + d, ks * s);
+        }
+      }
+#pragma unroll
+      for (int y = 0; y < FB; ++y) {
+#pragma unroll
+        for (int c = 0; c < FC; ++c) {
+          double s = 0.0;
+#pragma unroll
+          for (int x = 0; x < FA; ++x)
+#pragma unroll
+            for (int d = 0; d < FD; ++d)
+              s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoA + a_off + x) * N + kt.aoB + d];
+          atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, ks * s);
+        }
+#pragma unroll
+        for (int d = 0; d < FD; ++d) {
+          double s = 0.0;
+#pragma unroll
+          for (int x = 0; x < FA; ++x)
+#pragma unroll
+            for (int c = 0; c < FC; ++c)
+              s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoA + a_off + x) * N + kt.aoA + c];
+          atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoB + d, ks * s);
         }
       }
     }
-    R[0] = Fs[n];
   }
 }
 
-__host__ __device__ constexpr int cart_x(int l, int k) {
-  int s = 0;
-  while ((s + 1) * (s + 2) / 2 <= k) ++s;
-  return l - s;
-}
-__host__ __device__ constexpr int cart_z(int l, int k) {
-  int s = 0;
-  while ((s + 1) * (s + 2) / 2 <= k) ++s;
-  return k - s * (s + 1) / 2;
-}
-__host__ __device__ constexpr int cart_y(int l, int k) { return l - cart_x(l, k) - cart_z(l, k); }
+constexpr int kThreadBlock = 128;
+constexpr int kThreadWarps = kThreadBlock / 32;
 
-template <int LA, int LB, int LC, int LD, typename Tc>
-__global__ void __launch_bounds__(128) jk_thread_kernel(const JKArgs a) {
+template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH>
+__device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, const double *sph, Tc *ebra,
+                                               unsigned long long &cnt_q, unsigned long long &cnt_p,
+                                               unsigned long long &cnt_s) {
   constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-  constexpr int NAB = NA * NB, NCD = NC * ND;
+  constexpr int A0 = CH * NA / CA, A1 = (CH + 1) * NA / CA, NAc = A1 - A0;  // this chunk's A components
+  constexpr int NCD = NC * ND, NACC = NAc * NB * NCD;
   constexpr int N3L = n3(L);
   constexpr int EA = (LA + 1) * (LB + 1) * (LAB + 1), EC = (LC + 1) * (LD + 1) * (LCD + 1);
   constexpr bool SPH_NEEDED = (LA >= 2 || LB >= 2 || LC >= 2 || LD >= 2);
-  __shared__ double tab[kBoysTableDoubles];
-  __shared__ double sph[kSphTableDoubles];
-  for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
-  for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
-  __syncthreads();
+  constexpr int FAc = (LA >= 2) ? 2 * LA + 1 : NA, FBc = (LB >= 2) ? 2 * LB + 1 : NB;
+  constexpr int FCc = (LC >= 2) ? 2 * LC + 1 : NC, FDc = (LD >= 2) ? 2 * LD + 1 : ND;
+  // Buffer for the transformed chunk: spherical A (all m, partial sums) x B x C x D.
+  constexpr int NOUT = cmax(NACC, cmax(FAc, NAc) * cmax(NB, FBc) * cmax(NC, FCc) * cmax(ND, FDc));
   const int lane = threadIdx.x & 31;
-  const int N = a.nbf;
-  unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
+  const unsigned full = 0xffffffffu;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t base = a.q_begin + (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.nquartet;
        base += stride) {
@@ -83,9 +161,8 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(const JKArgs a) {
     const bool active = q < a.nquartet;
     int ib0 = 0;
     if (lane == 0) ib0 = find_bra(a.qoff, a.nbra, base);
-    ib0 = __shfl_sync(0xffffffffu, ib0, 0);
-    int ib = ib0, ic = 0;
-    int sel = 1;
+    ib0 = __shfl_sync(full, ib0, 0);
+    int ib = ib0, ic = 0, sel = 1;
     if (active) {
       int steps = 0;
       while (q >= a.qoff[ib + 1] && steps < 32) {
@@ -95,28 +172,38 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(const JKArgs a) {
       if (q >= a.qoff[ib + 1]) ib = find_bra(a.qoff, a.nbra, q);
       ic = (int)(q - a.qoff[ib]);
       sel = quartet_select(a, a.bra[ib], a.ket[ic]);
-      if (sel == 2) ++cnt_s;
+      if (sel == 2 && CH == 0) ++cnt_s;
     }
     const bool work = active && sel == 0;
-    double g[NAB * NCD];
+    Tc acc[NACC];
 #pragma unroll
-    for (int k = 0; k < NAB * NCD; ++k) g[k] = 0.0;
-    PairRec br, kt;
-    if (work) {
-      br = a.bra[ib];
-      kt = a.ket[ic];
-      Tc acc[NAB * NCD];
-#pragma unroll
-      for (int k = 0; k < NAB * NCD; ++k) acc[k] = Tc(0);
-      for (int i = 0; i < br.npp; ++i) {
-        const PrimPair P1 = a.pp[br.pp0 + i];
-        Tc ex1[EA], ey1[EA], ez1[EA];
-        const Tc h1 = Tc(0.5 / P1.p);
-        herm_e<LA, LB, 1, Tc>(h1, Tc(P1.PAx), Tc(P1.PBx), ex1);
-        herm_e<LA, LB, 1, Tc>(h1, Tc(P1.PAy), Tc(P1.PBy), ey1);
-        herm_e<LA, LB, 1, Tc>(h1, Tc(P1.PAz), Tc(P1.PBz), ez1);
+    for (int k = 0; k < NACC; ++k) acc[k] = Tc(0);
+    PairRec kt;
+    if (work) kt = a.ket[ic];
+    // Bra groups: lanes sharing a bra pair run its primitive loop together.
+    unsigned pending = __ballot_sync(full, work);
+    while (pending) {
+      const int leader = __ffs(pending) - 1;
+      const int ibl = __shfl_sync(full, ib, leader);
+      const bool mine = work && ib == ibl && ((pending >> lane) & 1u);
+      pending &= ~__ballot_sync(full, mine);
+      const PairRec brl = a.bra[ibl];
+      for (int i = 0; i < brl.npp; ++i) {
+        const PrimPair P1 = a.pp[brl.pp0 + i];
+        __syncwarp();
+        if (lane < 3) {
+          const Tc h1 = Tc(0.5 / P1.p);
+          const double pa = lane == 0 ? P1.PAx : lane == 1 ? P1.PAy : P1.PAz;
+          const double pb = lane == 0 ? P1.PBx : lane == 1 ? P1.PBy : P1.PBz;
+          herm_e<LA, LB, 1, Tc>(h1, Tc(pa), Tc(pb), ebra + lane * EA);
+        }
+        __syncwarp();
+        if (!mine) continue;
+        const Tc *ex1 = ebra, *ey1 = ebra + EA, *ez1 = ebra + 2 * EA;
+        PrimPair nxt = a.pp[kt.pp0];
         for (int j = 0; j < kt.npp; ++j) {
-          const PrimPair P2 = a.pp[kt.pp0 + j];
+          const PrimPair P2 = nxt;  // the next ket primitive pair is fetched during this one's arithmetic
+          if (j + 1 < kt.npp) nxt = a.pp[kt.pp0 + j + 1];
           const double rs = rsqrt(P1.p + P2.p);
           const double alpha = P1.p * P2.p * rs * rs;
           const double x = P1.Px - P2.Px, y = P1.Py - P2.Py, z = P1.Pz - P2.Pz;
@@ -164,7 +251,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(const JKArgs a) {
                           xk[tuv_index(t, u, v)] += e3 * R[tuv_index(t + ta, u + na, v + fa)];
                   }
 #pragma unroll
-              for (int ia = 0; ia < NA; ++ia)
+              for (int ia = A0; ia < A1; ++ia)
 #pragma unroll
                 for (int jb = 0; jb < NB; ++jb) {
                   const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
@@ -173,31 +260,32 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(const JKArgs a) {
 #pragma unroll
                   for (int t = 0; t <= ax + bx; ++t)
 #pragma unroll
-                    for (int u = 0; u <= ay + by; ++u)
+                    for (int u = 0; u <= ay + by; ++u) {
+                      const Tc exy = ex1[(ax * (LB + 1) + bx) * (LAB + 1) + t] * ey1[(ay * (LB + 1) + by) * (LAB + 1) + u];
 #pragma unroll
                       for (int v = 0; v <= az + bz; ++v)
-                        sum += ex1[(ax * (LB + 1) + bx) * (LAB + 1) + t] * ey1[(ay * (LB + 1) + by) * (LAB + 1) + u] *
-                               ez1[(az * (LB + 1) + bz) * (LAB + 1) + v] * xk[tuv_index(t, u, v)];
-                  acc[(ia * NB + jb) * NCD + c * ND + d] += sum;
+                        sum += exy * ez1[(az * (LB + 1) + bz) * (LAB + 1) + v] * xk[tuv_index(t, u, v)];
+                    }
+                  acc[((ia - A0) * NB + jb) * NCD + c * ND + d] += sum;
                 }
             }
         }
       }
-#pragma unroll
-      for (int k = 0; k < NAB * NCD; ++k) g[k] = (double)acc[k];
-      cnt_q += 1;
-      cnt_p += (unsigned long long)br.npp * kt.npp;
     }
-    // Cartesian -> spherical for d/f shells (in registers, compile-time sizes).
-    constexpr int FAc = (LA >= 2) ? 2 * LA + 1 : NA, FBc = (LB >= 2) ? 2 * LB + 1 : NB;
-    constexpr int FCc = (LC >= 2) ? 2 * LC + 1 : NC, FDc = (LD >= 2) ? 2 * LD + 1 : ND;
+    if (work) {
+      cnt_q += (CH == 0);
+      if (CH == 0) cnt_p += (unsigned long long)a.bra[ib].npp * kt.npp;
+    }
+    // Chunk block -> the shells' functions: spherical A (partial sums over
+    // this chunk's Cartesian components), then B, C, D.
     const bool sphr = SPH_NEEDED && a.spherical;
+    double g[NOUT];
+#pragma unroll
+    for (int k = 0; k < NOUT; ++k) g[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < NACC; ++k) g[k] = (double)acc[k];
     if (SPH_NEEDED && sphr && work) {
-      // index-by-index transform into a buffer of spherical sizes (<= Cartesian sizes)
-      double tmp[NAB * NCD];
-      constexpr int dims0[4] = {NA, NB, NC, ND};
-      int d0 = dims0[0], d1 = dims0[1], d2 = dims0[2], d3 = dims0[3];
-      (void)d0;
+      double tmp[NOUT];
       if (LA >= 2) {
         const double *T = sph + sph_offset(LA);
 #pragma unroll
@@ -206,17 +294,17 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(const JKArgs a) {
           for (int r = 0; r < NB * NCD; ++r) {
             double s = 0.0;
 #pragma unroll
-            for (int x = 0; x < NA; ++x) s += T[o * NA + x] * g[x * NB * NCD + r];
+            for (int x = 0; x < NAc; ++x) s += T[o * NA + A0 + x] * g[x * NB * NCD + r];
             tmp[o * NB * NCD + r] = s;
           }
 #pragma unroll
         for (int k = 0; k < FAc * NB * NCD; ++k) g[k] = tmp[k];
       }
-      constexpr int A1 = (LA >= 2) ? FAc : NA;
+      constexpr int A1r = (LA >= 2) ? FAc : NAc;
       if (LB >= 2) {
         const double *T = sph + sph_offset(LB);
 #pragma unroll
-        for (int i = 0; i < A1; ++i)
+        for (int i = 0; i < A1r; ++i)
 #pragma unroll
           for (int o = 0; o < FBc; ++o)
 #pragma unroll
@@ -227,9 +315,9 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(const JKArgs a) {
               tmp[(i * FBc + o) * NCD + r] = s;
             }
 #pragma unroll
-        for (int k = 0; k < A1 * FBc * NCD; ++k) g[k] = tmp[k];
+        for (int k = 0; k < A1r * FBc * NCD; ++k) g[k] = tmp[k];
       }
-      constexpr int AB1 = A1 * ((LB >= 2) ? FBc : NB);
+      constexpr int AB1 = A1r * ((LB >= 2) ? FBc : NB);
       if (LC >= 2) {
         const double *T = sph + sph_offset(LC);
 #pragma unroll
@@ -261,137 +349,43 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(const JKArgs a) {
 #pragma unroll
         for (int k = 0; k < ABC1 * FDc; ++k) g[k] = tmp[k];
       }
-      (void)d1;
-      (void)d2;
-      (void)d3;
     }
-    // Function counts of this launch (spherical or Cartesian basis).
-    const int FA = sphr ? FAc : NA, FB = sphr ? FBc : NB, FC = sphr ? FCc : NC, FD = sphr ? FDc : ND;
-    // Digestion: per slot, J_ab (warp-reduced when the warp shares its bra pair),
-    // J_cd, K_ac, K_ad, K_bc, K_bd as FP64 atomics into the half Fock matrices.
-    const unsigned full = 0xffffffffu;
+    // Digestion with compile-time function counts (spherical or Cartesian).
     const bool uniform = __all_sync(full, !work || ib == ib0) && __any_sync(full, work);
     if (!__any_sync(full, work)) continue;
-    double w = 0.0;
-    if (work) {
-      w = 1.0;
-      if (br.same) w *= 0.5;
-      if (kt.same) w *= 0.5;
-      if (a.same_class && ib == ic) w *= 0.5;
-    }
-    const PairRec brw = a.bra[ib0];
-    for (int k = 0; k < a.nslot; ++k) {
-      const double *Dk = a.D + (size_t)k * N * N;
-      const double *Dsk = a.Ds + (size_t)k * N * N;
-      double *Fk = a.Fh + (size_t)k * N * N;
-      const double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
-      if (a.jscale[k] != 0.0) {
-        // J_ab
-#pragma unroll
-        for (int x = 0; x < NA; ++x)
-#pragma unroll
-          for (int y = 0; y < NB; ++y) {
-            if (x >= FA || y >= FB) continue;
-            double s = 0.0;
-            if (work) {
-#pragma unroll
-              for (int c = 0; c < NC; ++c)
-#pragma unroll
-                for (int d = 0; d < ND; ++d)
-                  if (c < FC && d < FD)
-                    s += g[((x * FB + y) * FC + c) * FD + d] * Dsk[(size_t)(kt.aoA + c) * N + kt.aoB + d];
-              s *= js;
-            }
-            if (uniform) {
-#pragma unroll
-              for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(full, s, off);
-              if (lane == 0) atomicAdd(Fk + (size_t)(brw.aoA + x) * N + brw.aoB + y, s);
-            } else if (work) {
-              atomicAdd(Fk + (size_t)(br.aoA + x) * N + br.aoB + y, s);
-            }
-          }
-        if (work) {
-          // J_cd
-#pragma unroll
-          for (int c = 0; c < NC; ++c)
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-              if (c >= FC || d >= FD) continue;
-              double s = 0.0;
-#pragma unroll
-              for (int x = 0; x < NA; ++x)
-#pragma unroll
-                for (int y = 0; y < NB; ++y)
-                  if (x < FA && y < FB)
-                    s += g[((x * FB + y) * FC + c) * FD + d] * Dsk[(size_t)(br.aoA + x) * N + br.aoB + y];
-              atomicAdd(Fk + (size_t)(kt.aoA + c) * N + kt.aoB + d, js * s);
-            }
-        }
-      }
-      if (work && a.kscale[k] != 0.0) {
-        // K_ac and K_ad
-#pragma unroll
-        for (int x = 0; x < NA; ++x) {
-          if (x >= FA) continue;
-#pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            if (c >= FC) continue;
-            double s = 0.0;
-#pragma unroll
-            for (int y = 0; y < NB; ++y)
-#pragma unroll
-              for (int d = 0; d < ND; ++d)
-                if (y < FB && d < FD)
-                  s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoB + y) * N + kt.aoB + d];
-            atomicAdd(Fk + (size_t)(br.aoA + x) * N + kt.aoA + c, ks * s);
-          }
-#pragma unroll
-          for (int d = 0; d < ND; ++d) {
-            if (d >= FD) continue;
-            double s = 0.0;
-#pragma unroll
-            for (int y = 0; y < NB; ++y)
-#pragma unroll
-              for (int c = 0; c < NC; ++c)
-                if (y < FB && c < FC)
-                  s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoB + y) * N + kt.aoA + c];
-            atomicAdd(Fk + (size_t)(br.aoA + x) * N + kt.aoB + d, ks * s);
-          }
-        }
-        // K_bc and K_bd
-#pragma unroll
-        for (int y = 0; y < NB; ++y) {
-          if (y >= FB) continue;
-#pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            if (c >= FC) continue;
-            double s = 0.0;
-#pragma unroll
-            for (int x = 0; x < NA; ++x)
-#pragma unroll
-              for (int d = 0; d < ND; ++d)
-                if (x < FA && d < FD)
-                  s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoA + x) * N + kt.aoB + d];
-            atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, ks * s);
-          }
-#pragma unroll
-          for (int d = 0; d < ND; ++d) {
-            if (d >= FD) continue;
-            double s = 0.0;
-#pragma unroll
-            for (int x = 0; x < NA; ++x)
-#pragma unroll
-              for (int c = 0; c < NC; ++c)
-                if (x < FA && c < FC)
-                  s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoA + x) * N + kt.aoA + c];
-            atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoB + d, ks * s);
-          }
-        }
-      }
-    }
+    if (sphr)
+      jk_digest<FAc, FBc, FCc, FDc>(a, g, work, uniform, ib, ic, ib0, kt, 0);
+    else
+      jk_digest<NAc, NB, NC, ND>(a, g, work, uniform, ib, ic, ib0, kt, A0);
   }
-  // warp-aggregated counters
+}
+
+template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH>
+__device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, const double *tab, const double *sph,
+                                                   Tc *ebra, unsigned long long &q, unsigned long long &p,
+                                                   unsigned long long &s) {
+  if constexpr (CH < CA) {
+    if (chunk == CH)
+      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH>(a, tab, sph, ebra, q, p, s);
+    else
+      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1>(chunk, a, tab, sph, ebra, q, p, s);
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename Tc, int CA>
+__global__ void __launch_bounds__(kThreadBlock) jk_thread_kernel(const JKArgs a) {
+  constexpr int EA = (LA + 1) * (LB + 1) * (LA + LB + 1);
+  __shared__ double tab[kBoysTableDoubles];
+  __shared__ double sph[kSphTableDoubles];
+  __shared__ Tc ebra_all[kThreadWarps][3 * EA];
+  for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
+  for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
+  __syncthreads();
+  unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
+  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0>(blockIdx.y, a, tab, sph, ebra_all[threadIdx.x >> 5], cnt_q, cnt_p,
+                                                cnt_s);
   if (a.counters) {
+    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       cnt_q += __shfl_xor_sync(0xffffffffu, cnt_q, off);

@@ -102,4 +102,63 @@ __device__ __forceinline__ void herm_e(T h, T pa, T pb, T *E) {
   }
 }
 
+// Maps a flattened quartet index to (bra, ket) through the prefix array.
+__device__ __forceinline__ int find_bra(const int64_t *__restrict__ qoff, int nbra, int64_t q) {
+  int lo = 0, hi = nbra;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (qoff[mid] <= q)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// R_tuv for t+u+v <= L in place (compact index), from Fs[n] = pref (-2a)^n F_n:
+// level by level from n = L-1 down to 0, each level in decreasing t+u+v so
+// the level-(n+1) values it reads are still in place.
+template <int L, typename T>
+__device__ __forceinline__ void hermite_r_inplace(const T *Fs, T x, T y, T z, T *R) {
+  R[0] = Fs[L];
+#pragma unroll
+  for (int n = L - 1; n >= 0; --n) {
+#pragma unroll
+    for (int s = L - n; s >= 1; --s) {
+#pragma unroll
+      for (int w = 0; w <= s; ++w) {
+#pragma unroll
+        for (int v = 0; v <= w; ++v) {
+          const int u = w - v, t = s - w;
+          T val;
+          if (t > 0) {
+            val = x * R[tuv_index(t - 1, u, v)];
+            if (t > 1) val += T(t - 1) * R[tuv_index(t - 2, u, v)];
+          } else if (u > 0) {
+            val = y * R[tuv_index(t, u - 1, v)];
+            if (u > 1) val += T(u - 1) * R[tuv_index(t, u - 2, v)];
+          } else {
+            val = z * R[tuv_index(t, u, v - 1)];
+            if (v > 1) val += T(v - 1) * R[tuv_index(t, u, v - 2)];
+          }
+          R[tuv_index(t, u, v)] = val;
+        }
+      }
+    }
+    R[0] = Fs[n];
+  }
+}
+
+__host__ __device__ constexpr int cart_x(int l, int k) {
+  int s = 0;
+  while ((s + 1) * (s + 2) / 2 <= k) ++s;
+  return l - s;
+}
+__host__ __device__ constexpr int cart_z(int l, int k) {
+  int s = 0;
+  while ((s + 1) * (s + 2) / 2 <= k) ++s;
+  return k - s * (s + 1) / 2;
+}
+__host__ __device__ constexpr int cart_y(int l, int k) { return l - cart_x(l, k) - cart_z(l, k); }
+
 }  // namespace dgf

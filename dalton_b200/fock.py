@@ -117,6 +117,24 @@ class FockBuilder:
             self.last_stats = st.as_dict()
         return fmat
 
+    def autotune(self, dmat, thrs=1e-12, hfxfac=1.0):
+        """Time every candidate kernel per quartet class on this density (a
+        CUDA float64 tensor) and keep the fastest; returns the timing list."""
+        import json
+
+        import torch
+
+        d = dmat.contiguous()
+        opt = _lib.default_options(thrs=float(thrs), hfxfac=float(hfxfac))
+        buf = ctypes.create_string_buffer(1 << 16)
+        stream = torch.cuda.current_stream(d.device).cuda_stream
+        _lib.check(self._lib.dgf_autotune(self._h, ctypes.c_void_p(d.data_ptr()), ctypes.byref(opt),
+                                          ctypes.c_void_p(stream), buf, len(buf)), "dgf_autotune")
+        try:
+            return json.loads(buf.value.decode())
+        except ValueError:
+            return []
+
     def set_profiling(self, on: bool = True):
         _lib.check(self._lib.dgf_set_profiling(self._h, 1 if on else 0), "dgf_set_profiling")
 

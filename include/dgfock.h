@@ -174,6 +174,15 @@ int dgf_set_profiling(dgf_ctx *ctx, int on);
 /* Copy up to `max` records of the last profiled call; *count = records. */
 int dgf_get_profile(const dgf_ctx *ctx, dgf_class_time *out, int max, int *count);
 
+/* Per-class autotuner (no counterpart in Dalton): times every candidate
+ * kernel of every quartet class of the plan for opt->thrs on the density
+ * dmat_device (N x N, device) -- the cooperative team kernel and the
+ * thread-per-quartet kernel in its A-chunk variants, FP64 and FP32 -- and
+ * keeps the fastest per class and precision in the context for later builds.
+ * A JSON list of the timings is written to `report` (may be NULL). */
+int dgf_autotune(dgf_ctx *ctx, const double *dmat_device, const dgf_options *opt, void *stream, char *report,
+                 size_t report_len);
+
 /* Measurement helper (not part of the HERFCK contract): FP64 and FP32 FMA
  * throughput of device `device` in TFLOP/s from a register-resident FMA
  * loop, the denominator of the FP64-pipe roofline. */
