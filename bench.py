@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--scf-iters", type=int, default=12)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gradient", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run warmup+steps builds of a core-guess density (for ncu captures)")
     ap.add_argument("--mixed", action="store_true", help="with --profile-run: mixed form")
@@ -208,8 +209,71 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args):
+    """Batched J+K of many molecules: one graph-replayed launch sequence vs a
+    per-molecule launch loop (same contexts, same densities)."""
+    import torch
+
+    from dalton_b200 import molecules
+    from dalton_b200.basis import build_basis
+    from dalton_b200.batch import BatchBuilder
+    from dalton_b200.fock import FockBuilder
+
+    mols, basis = molecules.config(args.workload)
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    fbs = [FockBuilder(build_basis(m, basis)) for m in mols]
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    ds = []
+    for fb in fbs:  # a guess-like symmetric density (the Schwarz-screened quartet set does not depend on D)
+        d = rng.normal(size=(fb.nbf, fb.nbf)) * 1e-2
+        ds.append(torch.tensor(d + d.T + np.eye(fb.nbf) * 0.5, device=dev))
+    outs = [torch.empty_like(d) for d in ds]
+    bb = BatchBuilder(fbs)
+    dp = bb.pack(ds)
+    fp = torch.empty_like(dp)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    def loop():
+        for fb, d, o in zip(fbs, ds, outs):
+            fb.herfck_device(d, fmat=o, stats=False)
+
+    loop_ms = timed(loop)
+    graph_ms = timed(lambda: bb.herfck_batch(dp, fp, use_graph=True, stats=False))
+    nograph_ms = timed(lambda: bb.herfck_batch(dp, fp, use_graph=False, stats=False))
+    bb.herfck_batch(dp, fp, use_graph=True)
+    st = bb.last_stats
+    loop()
+    torch.cuda.synchronize(dev)
+    err = max(float(torch.max(torch.abs(a - b))) for a, b in zip(bb.unpack(fp), outs))
+    line = {"workload": f"{args.workload}: {len(mols)} water clusters of 1-16 molecules (seeded), {basis}, "
+                        f"{sum(fb.nbf for fb in fbs)} basis functions in all, J+K IFCTYP 13, Schwarz {THRS}",
+            "quartets": st["quartets_total"], "steps": args.steps, "warmup": args.warmup,
+            "per_molecule_loop_ms": loop_ms, "batched_graph_ms": graph_ms, "batched_no_graph_ms": nograph_ms,
+            "speedup_graph_vs_loop": loop_ms / graph_ms, "quartets_per_s_graph": st["quartets_total"] / (graph_ms * 1e-3),
+            "launches_batched": st["kernel_launches"], "max_abs_diff_vs_loop": err, "context_setup_s": setup_s,
+            "data": "synthetic (seeded clusters, guess-like densities)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload.startswith("batch") and args.impl != "reference":
+        run_batch(args)
+        return
     if args.profile_run:
         profile_run(args)
         return
@@ -366,6 +430,38 @@ def main():
     all_flops = sum(class_flops(r["la"], r["lb"], r["lc"], r["ld"], r["prim_quartets"], r["evaluated"]) for r in prof)
     build_tflops = all_flops / (tot_ms * 1e-3) / 1e12 if tot_ms else None
 
+    # HF nuclear gradient of (H2O)16 / cc-pVDZ (384 bf): backward kernel and full gradient.
+    grad_info = None
+    if not args.no_gradient and world == 1:
+        from dalton_b200.grad import grad2e_bilinear, rhf_gradient
+
+        gmol, gbas = molecules.config("h2o16_ccpvdz")
+        gbs = build_basis(gmol, gbas)
+        gfb = FockBuilder(gbs, device=local)
+        gscf = rhf(gbs, gfb, conv=1e-8, thrs=THRS)
+        Dg = gscf["dmat"].contiguous()
+        for _ in range(2):
+            grad2e_bilinear(gfb, Dg, Dg, 1.0, THRS)
+        torch.cuda.synchronize(dev)
+        gsteps = max(2, min(args.steps, 5))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(gsteps):
+            grad2e_bilinear(gfb, Dg, Dg, 1.0, THRS)
+        e1.record(stream)
+        e1.synchronize()
+        g2_ms = e0.elapsed_time(e1) / gsteps
+        t0 = time.perf_counter()
+        gfull = rhf_gradient(gfb, Dg, gscf["wmat"], thrs=THRS)
+        torch.cuda.synchronize(dev)
+        full_ms = (time.perf_counter() - t0) * 1e3
+        grad_info = {"workload": f"h2o16_ccpvdz: (H2O)16 cluster, {gbas}, {gbs.nbf} basis functions, RHF "
+                                 f"converged to 1e-8 ({gscf['niter']} iterations)",
+                     "grad2e_ms": g2_ms, "full_gradient_ms": full_ms, "energy": gscf["energy"],
+                     "max_abs_gradient": float(np.abs(gfull).max()),
+                     "translational_sum": float(np.abs(gfull.sum(0)).max())}
+        gfb.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(bs, D.cpu().numpy(), args.cpu_seconds)
@@ -394,6 +490,7 @@ def main():
             "autotune": {"seconds": tune_s, "candidates_timed": len(tuning)},
             "peaks_measured": {"fp64_tflops": fp64_peak, "fp32_tflops": fp32_peak},
             "gpu_launches": int((lmx if headline_mixed else l64)),
+            "hf_gradient": grad_info,
             "clocks": clk, "cpu_baseline": cpu,
             "profile_top": [{k: r[k] for k in ("la", "lb", "lc", "ld", "precision", "kernel", "evaluated",
                                                "prim_quartets", "ms")} for r in by_time[:8]],

@@ -20,7 +20,8 @@ DGF_OK, DGF_ERR_ARG, DGF_ERR_NOMEM, DGF_ERR_CUDA, DGF_ERR_UNSUPPORTED, DGF_ERR_T
 # Every symbol include/dgfock.h declares.
 EXPORTS = ["dgf_default_options", "dgf_create", "dgf_destroy", "dgf_fock", "dgf_fock_device", "dgf_grad2e",
            "dgf_grad2e_device", "dgf_grad2e_bilinear_device", "dgf_oneint", "dgf_grad1e", "dgf_set_profiling", "dgf_get_profile",
-           "dgf_measure_fma_peak", "dgf_autotune", "dgf_info", "dgf_strerror", "dgf_last_error"]
+           "dgf_measure_fma_peak", "dgf_autotune", "dgf_info", "dgf_strerror", "dgf_last_error",
+           "dgf_batch_create", "dgf_batch_destroy", "dgf_batch_layout", "dgf_fock_batch"]
 
 
 class DgfBasis(ctypes.Structure):
@@ -94,12 +95,12 @@ def load() -> ctypes.CDLL:
     lib.dgf_strerror.restype = ctypes.c_char_p
     lib.dgf_last_error.argtypes = []
     lib.dgf_last_error.restype = ctypes.c_char_p
-    if hasattr(lib, "dgf_batch_create"):
-        lib.dgf_batch_create.argtypes = [ctypes.POINTER(vp), dgf_int, ctypes.c_int, ctypes.POINTER(vp)]
-        lib.dgf_batch_destroy.argtypes = [vp]
-        lib.dgf_batch_destroy.restype = None
-        lib.dgf_fock_batch.argtypes = [vp, vp, vp, ctypes.POINTER(DgfOptions), ctypes.c_int, vp,
-                                       ctypes.POINTER(DgfStats)]
+    lib.dgf_batch_create.argtypes = [ctypes.POINTER(vp), dgf_int, ctypes.POINTER(vp)]
+    lib.dgf_batch_destroy.argtypes = [vp]
+    lib.dgf_batch_destroy.restype = None
+    lib.dgf_batch_layout.argtypes = [vp, _ip]
+    lib.dgf_fock_batch.argtypes = [vp, vp, vp, ctypes.POINTER(DgfOptions), ctypes.c_int, vp,
+                                   ctypes.POINTER(DgfStats)]
     _lib = lib
     return lib
 

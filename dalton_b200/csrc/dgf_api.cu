@@ -342,6 +342,7 @@ static JKArgs base_args(dgf_ctx *c) {
   a.spherical = c->spherical;
   a.nbf = c->nbf;
   a.nshell = c->nshell;
+  a.slot_stride = (int64_t)c->nbf * c->nbf;
   return a;
 }
 
@@ -467,6 +468,8 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
       r.same = (A == B);
       r.atA = c->sh_atom[sa];
       r.atB = c->sh_atom[sb];
+      r.nbfm = c->nbf;
+      r.dbase = 0;
       r.pp0 = (int)pp.size();
       for (int i = 0; i < c->sh_nprim[sa]; ++i)
         for (int j = 0; j < c->sh_nprim[sb]; ++j) {
@@ -519,10 +522,21 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
       cudaMemcpy(c->d_pairs, c->pairs.data(), c->pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice));
   int st = compute_schwarz(c.get());
   if (st) return st;
-  // Sort each class by Schwarz factor, descending, and re-upload.
-  for (int X = 0; X < kNumPairClass; ++X)
+  // Sort each class by (primitive-count bucket, Schwarz factor descending)
+  // and record the bucket boundaries, then re-upload.
+  for (int X = 0; X < kNumPairClass; ++X) {
     std::stable_sort(c->pairs.begin() + c->cls_off[X], c->pairs.begin() + c->cls_off[X + 1],
-                     [](const PairRec &u, const PairRec &v) { return u.Q > v.Q; });
+                     [](const PairRec &u, const PairRec &v) {
+                       const int bu = npp_bucket(u.npp), bv = npp_bucket(v.npp);
+                       return bu != bv ? bu < bv : u.Q > v.Q;
+                     });
+    const int n = c->cls_off[X + 1] - c->cls_off[X];
+    int pos = 0;
+    for (int b = 0; b <= kNumBuckets; ++b) {
+      while (b < kNumBuckets && pos < n && npp_bucket(c->pairs[c->cls_off[X] + pos].npp) < b) ++pos;
+      c->bkt_off[X][b] = (b == kNumBuckets) ? n : pos;
+    }
+  }
   DGF_CUDA_CHECK(
       cudaMemcpy(c->d_pairs, c->pairs.data(), c->pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice));
   *out = c.release();
@@ -551,29 +565,36 @@ static int build_plan(dgf_ctx *c, double thrs) {
       const int nb = c->cls_off[X + 1] - c->cls_off[X], nk = c->cls_off[Y + 1] - c->cls_off[Y];
       if (!nb || !nk) continue;
       const PairRec *bra = &c->pairs[c->cls_off[X]], *ket = &c->pairs[c->cls_off[Y]];
-      ClassPlan cp;
-      cp.X = X;
-      cp.Y = Y;
-      cp.off = (int64_t)all.size();
-      int64_t acc = 0;
-      all.push_back(0);
-      for (int i = 0; i < nb; ++i) {
-        const double qb = bra[i].Q;
-        int lo = 0, hi = nk;  // first ket with qb*Q < thrs
-        while (lo < hi) {
-          int mid = (lo + hi) >> 1;
-          if (qb * ket[mid].Q >= thrs)
-            lo = mid + 1;
-          else
-            hi = mid;
+      for (int kb = 0; kb < kNumBuckets; ++kb) {
+        const int k0 = c->bkt_off[Y][kb], k1 = c->bkt_off[Y][kb + 1];
+        if (k0 == k1) continue;
+        ClassPlan cp;
+        cp.X = X;
+        cp.Y = Y;
+        cp.kb0 = k0;
+        cp.kb1 = k1;
+        cp.off = (int64_t)all.size();
+        int64_t acc = 0;
+        all.push_back(0);
+        for (int i = 0; i < nb; ++i) {
+          const double qb = bra[i].Q;
+          int lo = k0, hi = k1;  // first ket of the bucket with qb*Q < thrs
+          while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (qb * ket[mid].Q >= thrs)
+              lo = mid + 1;
+            else
+              hi = mid;
+          }
+          int n = lo - k0;
+          // X == Y: canonical pairs, ket position <= bra position in the class order
+          if (X == Y) n = std::max(0, std::min(n, i - k0 + 1));
+          acc += n;
+          all.push_back(acc);
         }
-        int n = lo;
-        if (X == Y) n = std::min(n, i + 1);
-        acc += n;
-        all.push_back(acc);
+        cp.nquartet = acc;
+        if (acc > 0) plan.push_back(cp);
       }
-      cp.nquartet = acc;
-      if (acc > 0) plan.push_back(cp);
     }
   if (all.size() > c->qoff_cap) {
     if (c->d_qoff) cudaFree(c->d_qoff);
@@ -766,7 +787,8 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     a.mode = 0;
     for (const ClassPlan &cp : c->plan) {
       a.bra = c->d_pairs + c->cls_off[cp.X];
-      a.ket = c->d_pairs + c->cls_off[cp.Y];
+      a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
+      a.ket_off = cp.kb0;
       a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
       a.same_class = (cp.X == cp.Y);
       a.qoff = c->d_qoff + cp.off;
@@ -914,7 +936,11 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
   std::string rep = "[";
   const int saved_prof = c->profiling;
   c->profiling = 0;
-  for (const ClassPlan &cp : c->plan) {
+  // candidates are timed over all bucket entries of a class pair
+  for (size_t ip = 0; ip < c->plan.size();) {
+    size_t jp = ip;
+    while (jp < c->plan.size() && c->plan[jp].X == c->plan[ip].X && c->plan[jp].Y == c->plan[ip].Y) ++jp;
+    const ClassPlan &cp = c->plan[ip];
     JKArgs a = base_args(c);
     a.nslot = 1;
     a.D = c->d_D;
@@ -923,12 +949,9 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
     a.jscale[0] = 1.0;
     a.kscale[0] = 0.5 * o.hfxfac;
     a.bra = c->d_pairs + c->cls_off[cp.X];
-    a.ket = c->d_pairs + c->cls_off[cp.Y];
     a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
     a.same_class = (cp.X == cp.Y);
-    a.qoff = c->d_qoff + cp.off;
     a.q_begin = 0;
-    a.nquartet = cp.nquartet;
     const int la = cls_l1(cp.X), lb = cp.X - la * (la + 1) / 2, lc = cls_l1(cp.Y), ld = cp.Y - lc * (lc + 1) / 2;
     a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
     for (int p = 0; p < 2; ++p) {
@@ -938,10 +961,17 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
         const ClassKernel &k = jk_kernel_variant(cp.X, cp.Y, p, v);
         if (!k.launch) continue;
         float ms = 0.f;
-        for (int rep2 = 0; rep2 < 2; ++rep2) {  // first launch warms caches
+        for (int rep2 = 0; rep2 < 2; ++rep2) {  // first pass warms caches
           DGF_CUDA_CHECK(cudaEventRecord(e0, st));
-          r = launch_kernel(c, k, cp.X, cp.Y, a, st, p);
-          if (r) return r;
+          for (size_t q = ip; q < jp; ++q) {
+            const ClassPlan &cq = c->plan[q];
+            a.ket = c->d_pairs + c->cls_off[cq.Y] + cq.kb0;
+            a.ket_off = cq.kb0;
+            a.qoff = c->d_qoff + cq.off;
+            a.nquartet = cq.nquartet;
+            r = launch_kernel(c, k, cq.X, cq.Y, a, st, p);
+            if (r) return r;
+          }
           DGF_CUDA_CHECK(cudaEventRecord(e1, st));
           DGF_CUDA_CHECK(cudaEventSynchronize(e1));
           DGF_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
@@ -957,6 +987,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
       }
       c->choice[cp.X][cp.Y][p] = bestv;
     }
+    ip = jp;
   }
   c->profiling = saved_prof;
   rep += "]";

@@ -1,0 +1,409 @@
+// Batched Fock builds (pattern 2): many molecules of uneven size evaluated
+// by one launch per quartet class over a merged, class-sorted quartet queue,
+// the whole sequence captured once as a CUDA graph and replayed.
+//
+// Every molecule keeps its own canonical quartet list (no cross-molecule
+// quartets): the merged pair list of a class is the concatenation of the
+// molecules' Schwarz-sorted lists, each pair record carries its molecule's
+// offset and size in the packed D/F storage, and the plan stores, per bra
+// pair, the first ket of its molecule in the merged ket list.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dgf_ctx.h"
+#include "dgf_md.cuh"
+
+using namespace dgf;
+
+struct BatchPlan {
+  int X, Y;
+  int64_t off;       // into the qoff buffer (nbra+1 entries)
+  int64_t koff;      // into the kbase buffer (nbra entries)
+  int64_t nquartet;
+};
+
+struct dgf_batch {
+  int device = 0, nmol = 0, spherical = 1, nsm = 148;
+  std::vector<int64_t> offsets;  // nmol+1 packed offsets
+  std::vector<int> nbf;
+  int64_t total = 0;
+  std::vector<PairRec> pairs;
+  int cls_off[kNumPairClass + 1] = {0};
+  std::vector<int> mol_cls_off;  // [X * nmol + m]: start of molecule m's class-X pairs in the merged list
+  PairRec *d_pairs = nullptr;
+  PrimPair *d_pp = nullptr;
+  double *d_boys = nullptr, *d_sph = nullptr;
+  int64_t *d_offsets = nullptr;
+  int *d_nbf = nullptr;
+  double *d_D = nullptr, *d_Ds = nullptr, *d_Fh = nullptr;
+  unsigned long long *d_cnt = nullptr;
+  double plan_thrs = -1.0;
+  std::vector<BatchPlan> plan;
+  int64_t *d_qoff = nullptr;
+  int *d_kbase = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const double *g_in = nullptr;
+  double *g_out = nullptr;
+  double g_thrs = -1.0, g_hfx = 0.0;
+  cudaStream_t g_stream = nullptr;
+  int64_t launches = 0;
+};
+
+static void batch_free(dgf_batch *b) {
+  if (!b) return;
+  DeviceGuard g(b->device);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  void *ptrs[] = {b->d_pairs, b->d_pp, b->d_boys, b->d_sph, b->d_offsets, b->d_nbf, b->d_D, b->d_Ds, b->d_Fh,
+                  b->d_cnt, b->d_qoff, b->d_kbase};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+}
+
+#define BFAIL(code, msg)                       \
+  do {                                         \
+    ::dgf::set_error(__FILE__, __LINE__, msg); \
+    return code;                               \
+  } while (0)
+
+extern "C" void dgf_batch_destroy(dgf_batch *b) { batch_free(b); }
+
+extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **out) {
+  if (!out) BFAIL(DGF_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!ctxs || nmol <= 0) BFAIL(DGF_ERR_ARG, "empty batch");
+  for (dgf_int m = 0; m < nmol; ++m)
+    if (!ctxs[m]) BFAIL(DGF_ERR_ARG, "NULL context in batch");
+  const int dev = ctxs[0]->device, sph = ctxs[0]->spherical;
+  for (dgf_int m = 0; m < nmol; ++m)
+    if (ctxs[m]->device != dev || ctxs[m]->spherical != sph)
+      BFAIL(DGF_ERR_ARG, "batch contexts must share device and spherical flag");
+  dgf_batch *b = new dgf_batch;
+  b->device = dev;
+  b->nmol = (int)nmol;
+  b->spherical = sph;
+  b->nsm = ctxs[0]->nsm;
+  DeviceGuard g(dev);
+  b->offsets.assign(nmol + 1, 0);
+  for (dgf_int m = 0; m < nmol; ++m) {
+    b->nbf.push_back(ctxs[m]->nbf);
+    b->offsets[m + 1] = b->offsets[m] + (int64_t)ctxs[m]->nbf * ctxs[m]->nbf;
+  }
+  b->total = b->offsets[nmol];
+  std::vector<PrimPair> pp;
+  std::vector<int64_t> pp_off(nmol);
+  for (dgf_int m = 0; m < nmol; ++m) {
+    pp_off[m] = (int64_t)pp.size();
+    pp.insert(pp.end(), ctxs[m]->pp.begin(), ctxs[m]->pp.end());
+  }
+  if (pp.size() > (size_t)0x7fffffff) {
+    batch_free(b);
+    BFAIL(DGF_ERR_UNSUPPORTED, "batch too large (primitive pairs exceed 2^31)");
+  }
+  b->mol_cls_off.assign((size_t)kNumPairClass * nmol, 0);
+  for (int X = 0; X < kNumPairClass; ++X) {
+    b->cls_off[X] = (int)b->pairs.size();
+    for (dgf_int m = 0; m < nmol; ++m) {
+      const dgf_ctx *c = ctxs[m];
+      b->mol_cls_off[(size_t)X * nmol + m] = (int)b->pairs.size();
+      // The batch plan takes each bra's partners as a Schwarz prefix of its
+      // molecule's class list, so the list is ordered by Q alone here.
+      std::vector<PairRec> lst(c->pairs.begin() + c->cls_off[X], c->pairs.begin() + c->cls_off[X + 1]);
+      std::stable_sort(lst.begin(), lst.end(), [](const PairRec &u, const PairRec &v) { return u.Q > v.Q; });
+      for (const PairRec &src : lst) {
+        PairRec r = src;
+        r.pp0 += (int)pp_off[m];
+        r.nbfm = c->nbf;
+        r.dbase = b->offsets[m];
+        b->pairs.push_back(r);
+      }
+    }
+  }
+  b->cls_off[kNumPairClass] = (int)b->pairs.size();
+  const size_t n_boys = (size_t)(kBoysMaxM + 1) * kBoysTableDoubles;
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void **p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 8));
+  };
+  alloc((void **)&b->d_pairs, b->pairs.size() * sizeof(PairRec));
+  alloc((void **)&b->d_pp, pp.size() * sizeof(PrimPair));
+  alloc((void **)&b->d_boys, n_boys * 8);
+  alloc((void **)&b->d_sph, kSphTableDoubles * 8);
+  alloc((void **)&b->d_offsets, (nmol + 1) * 8);
+  alloc((void **)&b->d_nbf, nmol * 4);
+  alloc((void **)&b->d_D, b->total * 8);
+  alloc((void **)&b->d_Ds, b->total * 8);
+  alloc((void **)&b->d_Fh, b->total * 8);
+  alloc((void **)&b->d_cnt, 4 * kCounterSlots * 8);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    batch_free(b);
+    BFAIL(DGF_ERR_NOMEM, "device allocation for the batch failed");
+  }
+  e = cudaMemcpy(b->d_pairs, b->pairs.data(), b->pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_pp, pp.data(), pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_boys, ctxs[0]->d_boys, n_boys * 8, cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_sph, ctxs[0]->d_sph, kSphTableDoubles * 8, cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_offsets, b->offsets.data(), (nmol + 1) * 8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_nbf, b->nbf.data(), nmol * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+  if (e != cudaSuccess) {
+    std::string msg = cudaGetErrorString(e);
+    batch_free(b);
+    BFAIL(DGF_ERR_CUDA, msg);
+  }
+  *out = b;
+  return DGF_OK;
+}
+
+extern "C" int dgf_batch_layout(const dgf_batch *b, dgf_int *offsets) {
+  if (!b || !offsets) BFAIL(DGF_ERR_ARG, "NULL argument");
+  for (int m = 0; m <= b->nmol; ++m) offsets[m] = b->offsets[m];
+  return DGF_OK;
+}
+
+// Per-molecule quartet queues, merged per class pair.
+static int batch_plan(dgf_batch *b, double thrs) {
+  if (b->plan_thrs == thrs && !b->plan.empty()) return DGF_OK;
+  std::vector<int64_t> qoff;
+  std::vector<int> kbase;
+  std::vector<BatchPlan> plan;
+  const int nm = b->nmol;
+  auto mol_end = [&](int X, int m) {
+    return (m + 1 < nm) ? b->mol_cls_off[(size_t)X * nm + m + 1] : b->cls_off[X + 1];
+  };
+  for (int X = 0; X < kNumPairClass; ++X)
+    for (int Y = 0; Y <= X; ++Y) {
+      const int nb = b->cls_off[X + 1] - b->cls_off[X];
+      const int nk = b->cls_off[Y + 1] - b->cls_off[Y];
+      if (!nb || !nk) continue;
+      BatchPlan bp;
+      bp.X = X;
+      bp.Y = Y;
+      bp.off = (int64_t)qoff.size();
+      bp.koff = (int64_t)kbase.size();
+      int64_t acc = 0;
+      qoff.push_back(0);
+      for (int m = 0; m < nm; ++m) {
+        const int b0 = b->mol_cls_off[(size_t)X * nm + m], b1 = mol_end(X, m);
+        const int k0 = b->mol_cls_off[(size_t)Y * nm + m], k1 = mol_end(Y, m);
+        for (int i = b0; i < b1; ++i) {
+          const double qb = b->pairs[i].Q;
+          int lo = k0, hi = k1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (qb * b->pairs[mid].Q >= thrs)
+              lo = mid + 1;
+            else
+              hi = mid;
+          }
+          int n = lo - k0;
+          if (X == Y) n = std::min(n, i - b0 + 1);
+          acc += n;
+          qoff.push_back(acc);
+          kbase.push_back(k0 - b->cls_off[Y]);
+        }
+      }
+      bp.nquartet = acc;
+      if (acc > 0) plan.push_back(bp);
+    }
+  if (b->d_qoff) cudaFree(b->d_qoff);
+  if (b->d_kbase) cudaFree(b->d_kbase);
+  b->d_qoff = nullptr;
+  b->d_kbase = nullptr;
+  if (cudaMalloc(&b->d_qoff, std::max<size_t>(qoff.size(), 1) * 8) != cudaSuccess ||
+      cudaMalloc(&b->d_kbase, std::max<size_t>(kbase.size(), 1) * 4) != cudaSuccess) {
+    cudaGetLastError();
+    BFAIL(DGF_ERR_NOMEM, "device allocation of the batch plan failed");
+  }
+  if (cudaMemcpy(b->d_qoff, qoff.data(), qoff.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      (kbase.size() && cudaMemcpy(b->d_kbase, kbase.data(), kbase.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess))
+    BFAIL(DGF_ERR_CUDA, "upload of the batch plan failed");
+  b->plan.swap(plan);
+  b->plan_thrs = thrs;
+  if (b->exec) {  // a captured graph refers to the old plan
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+  return DGF_OK;
+}
+
+__device__ __forceinline__ int mol_of(const int64_t *__restrict__ off, int nmol, int64_t e) {
+  int lo = 0, hi = nmol;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= e)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Symmetric part of every packed density (IFCTYP 13): D = (D + D^T)/2, Ds = 2 D.
+__global__ void batch_prep_kernel(const double *__restrict__ Din, double *__restrict__ D, double *__restrict__ Ds,
+                                  const int64_t *__restrict__ off, const int *__restrict__ nbf, int nmol,
+                                  int64_t total) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int m = mol_of(off, nmol, e);
+    const int64_t base = off[m], loc = e - base;
+    const int n = nbf[m];
+    const int64_t p = loc / n, q = loc - p * n;
+    const double v = 0.5 * (Din[e] + Din[base + q * n + p]);
+    D[e] = v;
+    Ds[e] = 2.0 * v;
+  }
+}
+
+// F = Fh + Fh^T per packed block.
+__global__ void batch_combine_kernel(const double *__restrict__ Fh, double *__restrict__ F,
+                                     const int64_t *__restrict__ off, const int *__restrict__ nbf, int nmol,
+                                     int64_t total) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int m = mol_of(off, nmol, e);
+    const int64_t base = off[m], loc = e - base;
+    const int n = nbf[m];
+    const int64_t p = loc / n, q = loc - p * n;
+    F[e] = Fh[e] + Fh[base + q * n + p];
+  }
+}
+
+static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double hfx, cudaStream_t st) {
+  const int eb = 256;
+  const int eg = (int)std::max<int64_t>(1, std::min<int64_t>((b->total + eb - 1) / eb, (int64_t)b->nsm * 8));
+  int64_t launches = 0;
+  batch_prep_kernel<<<eg, eb, 0, st>>>(din, b->d_D, b->d_Ds, b->d_offsets, b->d_nbf, b->nmol, b->total);
+  ++launches;
+  if (cudaMemsetAsync(b->d_Fh, 0, b->total * 8, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "memset failed");
+  JKArgs a;
+  memset(&a, 0, sizeof(a));
+  a.pp = b->d_pp;
+  a.sph = b->d_sph;
+  a.spherical = b->spherical;
+  a.nslot = 1;
+  a.slot_stride = b->total;
+  a.D = b->d_D;
+  a.Ds = b->d_Ds;
+  a.Fh = b->d_Fh;
+  a.jscale[0] = 1.0;
+  a.kscale[0] = 0.5 * hfx;
+  int slot = 0;
+  for (const BatchPlan &bp : b->plan) {
+    a.bra = b->d_pairs + b->cls_off[bp.X];
+    a.ket = b->d_pairs + b->cls_off[bp.Y];
+    a.ket_off = 0;
+    a.nbra = b->cls_off[bp.X + 1] - b->cls_off[bp.X];
+    a.same_class = (bp.X == bp.Y);
+    a.qoff = b->d_qoff + bp.off;
+    a.kbase = b->d_kbase + bp.koff;
+    a.q_begin = 0;
+    a.nquartet = bp.nquartet;
+    a.counters = b->d_cnt + 4 * (slot++ % kCounterSlots);
+    const int la = (bp.X == 0) ? 0 : (bp.X <= 2) ? 1 : (bp.X <= 5) ? 2 : 3;
+    const int lb = bp.X - la * (la + 1) / 2;
+    const int lc = (bp.Y == 0) ? 0 : (bp.Y <= 2) ? 1 : (bp.Y <= 5) ? 2 : 3;
+    const int ld = bp.Y - lc * (lc + 1) / 2;
+    a.boys = b->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
+    const ClassKernel &k = jk_kernel(bp.X, bp.Y, 0);
+    const int64_t per_block = (k.smem == 0) ? k.block : 1;
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>((bp.nquartet + per_block - 1) / per_block, (int64_t)b->nsm * 16));
+    k.launch(a, grid, k.block, k.smem, st);
+    ++launches;
+  }
+  batch_combine_kernel<<<eg, eb, 0, st>>>(b->d_Fh, fout, b->d_offsets, b->d_nbf, b->nmol, b->total);
+  ++launches;
+  if (cudaGetLastError() != cudaSuccess) BFAIL(DGF_ERR_CUDA, "launch failed in the batched build");
+  b->launches = launches;
+  return DGF_OK;
+}
+
+extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, double *fmat_packed_device,
+                              const dgf_options *opt, int use_graph, void *stream, dgf_stats *stats) {
+  if (!b || !dmat_packed_device || !fmat_packed_device) BFAIL(DGF_ERR_ARG, "NULL argument");
+  DeviceGuard g(b->device);
+  dgf_options o;
+  dgf_default_options(&o);
+  if (opt) o = *opt;
+  if (o.ifthrs < 20 || o.mixed_cutoff > 0.0 || o.shard_count > 1)
+    BFAIL(DGF_ERR_UNSUPPORTED, "batched builds take the FP64 Schwarz-screened form only");
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  int r = batch_plan(b, o.thrs);
+  if (r) return r;
+  if (cudaMemsetAsync(b->d_cnt, 0, 4 * kCounterSlots * 8, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "memset failed");
+  if (cudaEventRecord(b->ev0, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "event record failed");
+  if (use_graph) {
+    const bool stale = !b->exec || b->g_in != dmat_packed_device || b->g_out != fmat_packed_device ||
+                       b->g_thrs != o.thrs || b->g_hfx != o.hfxfac || b->g_stream != st;
+    if (stale) {
+      if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+      }
+      // capture on the batch's own stream, replay on st (the counters are reset outside the graph)
+      cudaStream_t cs = b->stream;
+      if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        BFAIL(DGF_ERR_CUDA, "stream capture failed to begin");
+      r = batch_enqueue(b, dmat_packed_device, fmat_packed_device, o.hfxfac, cs);
+      cudaGraph_t gr = nullptr;
+      cudaError_t e = cudaStreamEndCapture(cs, &gr);
+      if (r) {
+        if (gr) cudaGraphDestroy(gr);
+        return r;
+      }
+      if (e != cudaSuccess) BFAIL(DGF_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&b->exec, gr, 0);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(gr);
+        BFAIL(DGF_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+      }
+      b->graph = gr;
+      b->g_in = dmat_packed_device;
+      b->g_out = fmat_packed_device;
+      b->g_thrs = o.thrs;
+      b->g_hfx = o.hfxfac;
+      b->g_stream = st;
+    }
+    if (cudaGraphLaunch(b->exec, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "graph launch failed");
+  } else {
+    r = batch_enqueue(b, dmat_packed_device, fmat_packed_device, o.hfxfac, st);
+    if (r) return r;
+  }
+  if (cudaEventRecord(b->ev1, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "event record failed");
+  if (stats) {
+    std::vector<unsigned long long> cnt(4 * kCounterSlots);
+    if (cudaMemcpyAsync(cnt.data(), b->d_cnt, cnt.size() * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      BFAIL(DGF_ERR_CUDA, "stats copy failed");
+    unsigned long long s[4] = {0, 0, 0, 0};
+    for (int i = 0; i < kCounterSlots; ++i)
+      for (int k = 0; k < 4; ++k) s[k] += cnt[4 * i + k];
+    int64_t tq = 0;
+    for (const BatchPlan &bp : b->plan) tq += bp.nquartet;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    stats->quartets_total = tq;
+    stats->quartets_fp64 = (int64_t)s[0];
+    stats->quartets_fp32 = 0;
+    stats->quartets_skipped = 0;
+    stats->prim_quartets = (int64_t)s[1];
+    stats->kernel_launches = b->launches;
+    stats->ms_device = ms;
+  }
+  return DGF_OK;
+}

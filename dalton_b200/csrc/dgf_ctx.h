@@ -2,13 +2,25 @@
 // shell-pair data and the per-call scratch of one molecule/basis.
 #pragma once
 
+#include "../../include/dgfock.h"
 #include "dgf_internal.h"
+
+#define DGF_CUDA_CHECK(expr)                                                   \
+  do {                                                                         \
+    cudaError_t _e = (expr);                                                   \
+    if (_e != cudaSuccess) {                                                   \
+      ::dgf::set_error(__FILE__, __LINE__, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+      return DGF_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)
+
 
 constexpr int kCounterSlots = 256;
 
 struct ClassPlan {
   int X, Y;
-  int64_t off;        // offset of this class pair's qoff array in the plan buffer
+  int kb0, kb1;       // ket range of this entry: one primitive-count bucket of class Y (relative to its start)
+  int64_t off;        // offset of this entry's qoff array in the plan buffer
   int64_t nquartet;
 };
 
@@ -19,6 +31,8 @@ struct dgf_ctx {
   std::vector<double> sh_a, sh_c;
   std::vector<dgf::PairRec> pairs;  // class-major, Schwarz-descending inside a class
   int cls_off[dgf::kNumPairClass + 1] = {0};
+  // per class: bucket boundaries (relative to the class start), pairs sorted by (bucket, -Q)
+  int bkt_off[dgf::kNumPairClass][dgf::kNumBuckets + 1] = {};
   std::vector<dgf::PrimPair> pp;
   dgf::PairRec *d_pairs = nullptr;
   dgf::PrimPair *d_pp = nullptr;

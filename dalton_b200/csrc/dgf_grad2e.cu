@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) grad_thread_kernel(const JKArgs a) {
     double w = 1.0;
     if (br.same) w *= 0.5;
     if (kt.same) w *= 0.5;
-    if (a.same_class && ib == ic) w *= 0.5;
+    if (a.same_class && ib == ic + a.ket_off) w *= 0.5;
     // Density product in the shells' own functions, then back to Cartesians.
     const int fa = sphr ? FA : NA, fb = sphr ? FB : NB, fc = sphr ? FC : NC, fd = sphr ? FD : ND;
     double G[NAB * NCD];
@@ -302,7 +302,8 @@ static int grad_impl(dgf_ctx *c, const double *d1, const double *d2, double hfx,
   a.hfx = hfx;
   for (const ClassPlan &cp : c->plan) {
     a.bra = c->d_pairs + c->cls_off[cp.X];
-    a.ket = c->d_pairs + c->cls_off[cp.Y];
+    a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
+    a.ket_off = cp.kb0;
     a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
     a.same_class = (cp.X == cp.Y);
     a.qoff = c->d_qoff + cp.off;

@@ -8,13 +8,19 @@
 #include <string>
 #include <vector>
 
-#include "../../include/dgfock.h"
 
 namespace dgf {
 
 constexpr int kMaxShellL = 3;                                         // s, p, d, f
 constexpr int kNumPairClass = (kMaxShellL + 1) * (kMaxShellL + 2) / 2;  // (la >= lb) classes
 constexpr int kMaxSlots = 8;  // density slots processed together by one kernel pass
+constexpr int kNumBuckets = 7;  // primitive-pair-count buckets of a class list
+
+// Bucket of a pair by its primitive-pair count (1, 2, <=4, <=8, <=16, <=32, more):
+// lanes of a warp then loop over similar ket primitive counts.
+__host__ __device__ inline int npp_bucket(int n) {
+  return n <= 1 ? 0 : n <= 2 ? 1 : n <= 4 ? 2 : n <= 8 ? 3 : n <= 16 ? 4 : n <= 32 ? 5 : 6;
+}
 
 // Boys-function table: F_M(T) on [0, kBoysTmax) in kBoysNint intervals of
 // width 1/kBoysPerUnit, a degree-kBoysDeg polynomial in x = (T - mid) * 2 *
@@ -42,12 +48,14 @@ struct PrimPair {
 // Shell pair record in a class list (sorted by Schwarz factor, descending).
 struct PairRec {
   int shA, shB;    // segmented shell indices (A has l >= l of B)
-  int aoA, aoB;    // first AO of each shell
+  int aoA, aoB;    // first AO of each shell (within its molecule)
   int pp0, npp;    // primitive-pair range
   int same;        // A == B
   int atA;         // atom of A (atom of B in atB)
-  int atB, pad;
+  int atB;
+  int nbfm;        // basis size of the pair's molecule (row stride of its D/F blocks)
   double Q;        // Schwarz factor sqrt(max |(ab|ab)|)
+  int64_t dbase;   // offset of the molecule's N x N block in packed D/F storage (0 for one molecule)
 };
 
 // Arguments of one quartet-class launch.
@@ -55,6 +63,9 @@ struct JKArgs {
   const PairRec *bra;
   const PairRec *ket;
   const int64_t *qoff;      // prefix sums of ket partners per bra (nbra+1), device
+  const int *kbase;         // per bra: first ket of its molecule in the ket list (batches), or null
+  int ket_off;              // position of ket[0] in its class list (same-class weight compares ib, ic + ket_off)
+  int64_t slot_stride;      // elements between density slots in D, Ds, Fh
   int nbra;
   int same_class;           // bra class == ket class (canonical ket <= bra)
   int64_t q_begin;          // first quartet of this launch (shard start)
@@ -119,11 +130,3 @@ void set_error(const char *file, int line, const std::string &msg);
 
 }  // namespace dgf
 
-#define DGF_CUDA_CHECK(expr)                                                   \
-  do {                                                                         \
-    cudaError_t _e = (expr);                                                   \
-    if (_e != cudaSuccess) {                                                   \
-      ::dgf::set_error(__FILE__, __LINE__, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
-      return DGF_ERR_CUDA;                                                     \
-    }                                                                          \
-  } while (0)

@@ -92,7 +92,6 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
     tuv_decode(e, t, u, v);
     tuvt[e] = t | (u << 8) | (v << 16);
   }
-  const int N = a.nbf;
   const int FA = nfun(LA, a.spherical), FB = nfun(LB, a.spherical);
   const int FC = nfun(LC, a.spherical), FD = nfun(LD, a.spherical);
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
@@ -105,7 +104,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
         ib = ic = (int)q;
       } else {
         ib = find_bra(a.qoff, a.nbra, q);
-        ic = (int)(q - a.qoff[ib]);
+        ic = (int)(q - a.qoff[ib]) + (a.kbase ? a.kbase[ib] : 0);
       }
       s_ib = ib;
       s_ic = ic;
@@ -114,7 +113,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
       double w = 1.0;
       if (br.same) w *= 0.5;
       if (kt.same) w *= 0.5;
-      if (a.same_class && ib == ic) w *= 0.5;
+      if (a.same_class && ib == ic + a.ket_off) w *= 0.5;
       s_w = w;
     }
     __syncthreads();
@@ -261,11 +260,13 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
 
     const double w = s_w;
     const int aoA = br.aoA, aoB = br.aoB, aoC = kt.aoA, aoD = kt.aoB;
+    const int64_t db = kt.dbase;
+    const int N = kt.nbfm;
     double *Dcd = dst, *Dab = dst + 100, *Dbd = dst + 200, *Dbc = dst + 300, *Dad = dst + 400, *Dac = dst + 500;
     for (int k = 0; k < a.nslot; ++k) {
-      const double *Dk = a.D + (size_t)k * N * N;
-      const double *Dsk = a.Ds + (size_t)k * N * N;
-      double *Fk = a.Fh + (size_t)k * N * N;
+      const double *Dk = a.D + k * a.slot_stride + db;
+      const double *Dsk = a.Ds + k * a.slot_stride + db;
+      double *Fk = a.Fh + k * a.slot_stride + db;
       const double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
       for (int e = tid; e < 100; e += nt) {
         int r = e / 10, c = e % 10;

@@ -30,7 +30,6 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
                                           int ib0, const PairRec &kt, int a_off) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int N = a.nbf;
   double w = 0.0;
   PairRec br;
   if (work) {
@@ -38,13 +37,19 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
     w = 1.0;
     if (br.same) w *= 0.5;
     if (kt.same) w *= 0.5;
-    if (a.same_class && ib == ic) w *= 0.5;
+    if (a.same_class && ib == ic + a.ket_off) w *= 0.5;
   }
+  // The warp's bra pair (valid on every lane) for the warp-reduced J_ab block;
+  // a quartet's bra and ket belong to one molecule, so its N x N block is
+  // the bra's.
   const PairRec brw = a.bra[ib0];
+  const int N = work ? br.nbfm : brw.nbfm;
+  const int64_t db = work ? br.dbase : brw.dbase;
   for (int k = 0; k < a.nslot; ++k) {
-    const double *Dk = a.D + (size_t)k * N * N;
-    const double *Dsk = a.Ds + (size_t)k * N * N;
-    double *Fk = a.Fh + (size_t)k * N * N;
+    const double *Dk = a.D + k * a.slot_stride + db;
+    const double *Dsk = a.Ds + k * a.slot_stride + db;
+    double *Fk = a.Fh + k * a.slot_stride + db;
+    double *Fw = a.Fh + k * a.slot_stride + brw.dbase;
     const double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
     if (a.jscale[k] != 0.0) {
 #pragma unroll
@@ -63,7 +68,7 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
           if (uniform) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(full, s, off);
-            if (lane == 0) atomicAdd(Fk + (size_t)(brw.aoA + a_off + x) * N + brw.aoB + y, s);
+            if (lane == 0) atomicAdd(Fw + (size_t)(brw.aoA + a_off + x) * brw.nbfm + brw.aoB + y, s);
           } else if (work) {
             atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + br.aoB + y, s);
           }
@@ -170,7 +175,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
         ++steps;
       }
       if (q >= a.qoff[ib + 1]) ib = find_bra(a.qoff, a.nbra, q);
-      ic = (int)(q - a.qoff[ib]);
+      ic = (int)(q - a.qoff[ib]) + (a.kbase ? a.kbase[ib] : 0);
       sel = quartet_select(a, a.bra[ib], a.ket[ic]);
       if (sel == 2 && CH == 0) ++cnt_s;
     }

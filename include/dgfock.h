@@ -174,6 +174,26 @@ int dgf_set_profiling(dgf_ctx *ctx, int on);
 /* Copy up to `max` records of the last profiled call; *count = records. */
 int dgf_get_profile(const dgf_ctx *ctx, dgf_class_time *out, int max, int *count);
 
+/* Batched Fock builds of many molecules (no counterpart in Dalton, which
+ * builds one molecule per run): one launch per quartet class covers every
+ * molecule's canonical quartet queue, merged class by class; the launch
+ * sequence can be captured once as a CUDA graph and replayed.  Contexts must
+ * live on one device with the same spherical flag and stay alive while the
+ * batch exists.  Matrices are packed: molecule k's N_k x N_k block starts at
+ * offsets[k] (offsets[nmol] = total doubles), see dgf_batch_layout. */
+typedef struct dgf_batch dgf_batch;
+int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **out);
+void dgf_batch_destroy(dgf_batch *batch);
+int dgf_batch_layout(const dgf_batch *batch, dgf_int *offsets /* nmol + 1 */);
+
+/* J+K (IFCTYP 13, HFXFAC from opt) of every molecule of the batch, device
+ * pointers to packed D and F.  use_graph = 1: the first call captures the
+ * launch sequence into a CUDA graph, later calls with the same pointers,
+ * options and stream replay it.  Only the FP64 Schwarz-screened form
+ * (ifthrs >= 20, mixed_cutoff = 0, one shard). */
+int dgf_fock_batch(dgf_batch *batch, const double *dmat_packed_device, double *fmat_packed_device,
+                   const dgf_options *opt, int use_graph, void *stream, dgf_stats *stats);
+
 /* Per-class autotuner (no counterpart in Dalton): times every candidate
  * kernel of every quartet class of the plan for opt->thrs on the density
  * dmat_device (N x N, device) -- the cooperative team kernel and the
