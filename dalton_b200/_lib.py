@@ -21,7 +21,8 @@ DGF_OK, DGF_ERR_ARG, DGF_ERR_NOMEM, DGF_ERR_CUDA, DGF_ERR_UNSUPPORTED, DGF_ERR_T
 EXPORTS = ["dgf_default_options", "dgf_create", "dgf_destroy", "dgf_fock", "dgf_fock_device", "dgf_grad2e",
            "dgf_grad2e_device", "dgf_grad2e_bilinear_device", "dgf_oneint", "dgf_grad1e", "dgf_set_profiling", "dgf_get_profile",
            "dgf_measure_fma_peak", "dgf_autotune", "dgf_info", "dgf_strerror", "dgf_last_error",
-           "dgf_batch_create", "dgf_batch_destroy", "dgf_batch_layout", "dgf_fock_batch"]
+           "dgf_batch_create", "dgf_batch_destroy", "dgf_batch_layout", "dgf_fock_batch",
+           "dgf_fock_device_noalloc"]
 
 
 class DgfBasis(ctypes.Structure):

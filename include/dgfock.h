@@ -126,6 +126,25 @@ int dgf_fock(dgf_ctx *ctx, dgf_int ndmat, const dgf_int *ifctyp, const double *d
 int dgf_fock_device(dgf_ctx *ctx, dgf_int ndmat, const dgf_int *ifctyp, const double *dmat_device,
                     double *fmat_device, const dgf_options *opt, void *stream, dgf_stats *stats);
 
+/* Fock build that allocates no device memory.  No counterpart in Dalton:
+ * an addition for callers that cannot allocate GPU memory when they need a
+ * Fock matrix, such as a host that, like Dalton, gives the engine one fixed
+ * work area and nothing more, or a process whose device memory is owned by
+ * another pool.  Same result as dgf_fock_device with ndmat = 1, IFCTYP 13,
+ * ifthrs >= 20, mixed_cutoff = 0: F = J[D] - hfxfac/2 K[D] of one density
+ * (symmetrised), device pointers.  Its scratch is a fixed device array of
+ * 3 x 768 x 768 doubles (14.2 MB) that every GPU loading this library holds
+ * until exit; contexts with more than 768 basis functions are rejected
+ * (DGF_ERR_ARG).  The context's quartet plan for `thrs` must exist already
+ * (an earlier dgf_fock, dgf_fock_device, dgf_autotune or dgf_grad2e call
+ * with this threshold builds it), else DGF_ERR_ARG.  The first call on a
+ * device looks up the array's device address; make it before any CUDA
+ * stream capture.  All calls share the array and leave its contents behind;
+ * calls that overlap on the GPU (other streams or host threads) race and
+ * must be serialised by the caller. */
+int dgf_fock_device_noalloc(dgf_ctx *ctx, const double *dmat_device, double *fmat_device, double hfxfac,
+                            double thrs, void *stream);
+
 /* Two-electron part of the RHF nuclear gradient (TWOEXP -> INTEX1 -> DEROUT,
  * aba2tex.F:242, her2ave.F:91-830): grad(natom,3) is overwritten with
  *   1/2 sum_pqrs d(pq|rs)/dx [D_pq D_rs - hfxfac/2 D_pr D_qs],
