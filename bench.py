@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--profile-run", action="store_true",
                     help="only run warmup+steps builds of a core-guess density (for ncu captures)")
     ap.add_argument("--mixed", action="store_true", help="with --profile-run: mixed form")
+    ap.add_argument("--grad", action="store_true", help="with --profile-run: the two-electron gradient kernels")
     return ap.parse_args()
 
 
@@ -71,8 +72,14 @@ def profile_run(args):
     C = X @ C
     nocc = mol.nelectrons() // 2
     D = (2.0 * C[:, :nocc] @ C[:, :nocc].T).contiguous()
-    for _ in range(args.warmup + args.steps):
-        fb.herfck_device(D, ifctyp=13, thrs=THRS, mixed_cutoff=MIXED_CUTOFF if args.mixed else 0.0)
+    if args.grad:
+        from dalton_b200.grad import grad2e_bilinear
+
+        for _ in range(args.warmup + args.steps):
+            grad2e_bilinear(fb, D, D, 1.0, THRS)
+    else:
+        for _ in range(args.warmup + args.steps):
+            fb.herfck_device(D, ifctyp=13, thrs=THRS, mixed_cutoff=MIXED_CUTOFF if args.mixed else 0.0)
     torch.cuda.synchronize()
     print(json.dumps({"profile_run": args.workload, "builds": args.warmup + args.steps, "stats": fb.last_stats}))
 

@@ -73,39 +73,42 @@ double boys_reference(int m, double t) {
 // Chebyshev interpolant of F_M on each interval at kBoysNcoef nodes, written
 // out as a polynomial in the interval's local variable x in [-1, 1].
 void boys_table_host(std::vector<double> &out) {
-  const int n = kBoysNcoef;
   const long double pi = 3.14159265358979323846264338327950288L;
-  out.assign((size_t)(kBoysMaxM + 1) * kBoysTableDoubles, 0.0);
-  std::vector<long double> f(n), c(n), tk(n * n), pw(n);
-  // monomial coefficients of T_j(x): tk[j*n + k]
-  std::fill(tk.begin(), tk.end(), 0.0L);
-  tk[0] = 1.0L;
-  if (n > 1) tk[1 * n + 1] = 1.0L;
-  for (int j = 2; j < n; ++j)
-    for (int k = 0; k < n; ++k) {
-      long double v = -tk[(j - 2) * n + k];
-      if (k > 0) v += 2.0L * tk[(j - 1) * n + k - 1];
-      tk[j * n + k] = v;
-    }
+  out.assign(kBoysAllDoubles, 0.0);
   const long double h = 1.0L / kBoysPerUnit;
-  for (int M = 0; M <= kBoysMaxM; ++M)
-    for (int i = 0; i < kBoysNint; ++i) {
-      const long double mid = (i + 0.5L) * h;
+  // Two table sets: full degree kBoysDeg and low degree kBoysDegLow.
+  for (int set = 0; set < 2; ++set) {
+    const int n = (set == 0 ? kBoysDeg : kBoysDegLow) + 1;
+    std::vector<long double> f(n), c(n), tk(n * n, 0.0L), pw(n);
+    // monomial coefficients of T_j(x): tk[j*n + k]
+    tk[0] = 1.0L;
+    if (n > 1) tk[1 * n + 1] = 1.0L;
+    for (int j = 2; j < n; ++j)
       for (int k = 0; k < n; ++k) {
-        long double x = cosl(pi * (k + 0.5L) / n);
-        f[k] = boys_series(M, mid + 0.5L * h * x);
+        long double v = -tk[(j - 2) * n + k];
+        if (k > 0) v += 2.0L * tk[(j - 1) * n + k - 1];
+        tk[j * n + k] = v;
       }
-      for (int j = 0; j < n; ++j) {
-        long double s = 0;
-        for (int k = 0; k < n; ++k) s += f[k] * cosl(pi * j * (k + 0.5L) / n);
-        c[j] = s * 2.0L / n;
+    for (int M = 0; M <= kBoysMaxM; ++M)
+      for (int i = 0; i < kBoysNint; ++i) {
+        const long double mid = (i + 0.5L) * h;
+        for (int k = 0; k < n; ++k) {
+          long double x = cosl(pi * (k + 0.5L) / n);
+          f[k] = boys_series(M, mid + 0.5L * h * x);
+        }
+        for (int j = 0; j < n; ++j) {
+          long double sm = 0;
+          for (int k = 0; k < n; ++k) sm += f[k] * cosl(pi * j * (k + 0.5L) / n);
+          c[j] = sm * 2.0L / n;
+        }
+        c[0] *= 0.5L;
+        std::fill(pw.begin(), pw.end(), 0.0L);
+        for (int j = 0; j < n; ++j)
+          for (int k = 0; k < n; ++k) pw[k] += c[j] * tk[j * n + k];
+        const size_t base = (set == 0 ? (size_t)M * kBoysTableDoubles : boys_low_offset(M)) + (size_t)i * kBoysNcoef;
+        for (int k = 0; k < n; ++k) out[base + k] = (double)pw[k];
       }
-      c[0] *= 0.5L;
-      std::fill(pw.begin(), pw.end(), 0.0L);
-      for (int j = 0; j < n; ++j)
-        for (int k = 0; k < n; ++k) pw[k] += c[j] * tk[j * n + k];
-      for (int k = 0; k < n; ++k) out[(size_t)M * kBoysTableDoubles + i * n + k] = (double)pw[k];
-    }
+  }
 }
 
 // Cartesian -> real spherical coefficients with Dalton's conventions (SPHCO1,
@@ -801,8 +804,11 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
       const int ld = cp.Y - lc * (lc + 1) / 2;
       a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
       const bool split = o.mixed_cutoff > 0.0 && jk_kernel(cp.X, cp.Y, 1).launch != nullptr;
+      const int Lq = la + lb + lc + ld;
       for (int part = 0; part < (split ? 2 : 1); ++part) {
         a.mode = split ? 1 + part : 0;
+        // the FP32 half reads the low-degree Boys table
+        a.boys = c->d_boys + ((split && part == 1) ? boys_low_offset(Lq) : (size_t)Lq * kBoysTableDoubles);
         a.counters = c->d_cnt + 4 * (nlaunch_class % kCounterSlots);
         ++nlaunch_class;
         int r = launch_class(c, cp.X, cp.Y, a, st, split && part == 1 ? 1 : 0);
@@ -957,6 +963,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
     for (int p = 0; p < 2; ++p) {
       float best = 1e30f;
       int bestv = c->choice[cp.X][cp.Y][p];
+      a.boys = c->d_boys + (p ? boys_low_offset(la + lb + lc + ld) : (size_t)(la + lb + lc + ld) * kBoysTableDoubles);
       for (int v = -1; v < kThreadVariants; ++v) {
         const ClassKernel &k = jk_kernel_variant(cp.X, cp.Y, p, v);
         if (!k.launch) continue;

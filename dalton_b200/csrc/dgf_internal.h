@@ -32,6 +32,13 @@ constexpr int kBoysNint = 80;
 constexpr int kBoysDeg = 11;
 constexpr int kBoysNcoef = kBoysDeg + 1;
 constexpr int kBoysTableDoubles = kBoysNint * kBoysNcoef;
+constexpr int kBoysDegLow = 5;  // tables of the FP32 half of the mixed form
+// Device table layout: orders 0..kBoysMaxM at full degree, then the same
+// orders at degree kBoysDegLow (same interval layout, unused coefficients 0).
+constexpr size_t kBoysAllDoubles = 2 * (size_t)(kBoysMaxM + 1) * kBoysTableDoubles;
+__host__ __device__ constexpr size_t boys_low_offset(int M) {
+  return ((size_t)(kBoysMaxM + 1) + M) * kBoysTableDoubles;
+}
 
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 __host__ __device__ constexpr int n3(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }

@@ -205,15 +205,14 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
         __syncwarp();
         if (!mine) continue;
         const Tc *ex1 = ebra, *ey1 = ebra + EA, *ez1 = ebra + 2 * EA;
-        PrimPair nxt = a.pp[kt.pp0];
-        for (int j = 0; j < kt.npp; ++j) {
-          const PrimPair P2 = nxt;  // the next ket primitive pair is fetched during this one's arithmetic
-          if (j + 1 < kt.npp) nxt = a.pp[kt.pp0 + j + 1];
-          const double rs = rsqrt(P1.p + P2.p);
+        // One ket primitive pair (a zero K makes it contribute nothing).
+        auto ket_prim = [&](const PrimPair &P2) {
+          // FP32 half: FP32 rsqrt for the prefactor and the low-degree FP64 Boys table
+          const double rs = (sizeof(Tc) == 4) ? (double)rsqrtf((float)(P1.p + P2.p)) : rsqrt(P1.p + P2.p);
           const double alpha = P1.p * P2.p * rs * rs;
           const double x = P1.Px - P2.Px, y = P1.Py - P2.Py, z = P1.Pz - P2.Pz;
           double F[L + 1];
-          boys_eval<L>(alpha * (x * x + y * y + z * z), tab, F);
+          boys_eval<L, (sizeof(Tc) == 4) ? kBoysDegLow : kBoysDeg>(alpha * (x * x + y * y + z * z), tab, F);
           Tc Fs[L + 1];
           double s = P1.K * P2.K * rs;
 #pragma unroll
@@ -274,6 +273,26 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
                   acc[((ia - A0) * NB + jb) * NCD + c * ND + d] += sum;
                 }
             }
+        };
+        if constexpr (L <= 2) {
+          // two independent primitive quartets per iteration for latency hiding
+          for (int j = 0; j < kt.npp; j += 2) {
+            const PrimPair P2a = a.pp[kt.pp0 + j];
+            PrimPair P2b = P2a;
+            if (j + 1 < kt.npp)
+              P2b = a.pp[kt.pp0 + j + 1];
+            else
+              P2b.K = 0.0;
+            ket_prim(P2a);
+            ket_prim(P2b);
+          }
+        } else {
+          PrimPair nxt = a.pp[kt.pp0];
+          for (int j = 0; j < kt.npp; ++j) {
+            const PrimPair P2 = nxt;  // the next ket primitive pair is fetched during this one's arithmetic
+            if (j + 1 < kt.npp) nxt = a.pp[kt.pp0 + j + 1];
+            ket_prim(P2);
+          }
         }
       }
     }

@@ -38,19 +38,34 @@ __host__ __device__ __forceinline__ void cart_decode(int l, int k, int &x, int &
   x = l - s;
 }
 
+// Polynomial of degree DEG in x (coefficients c[0..DEG]) by Estrin's scheme:
+// the dependency depth grows with log2(DEG) instead of DEG.
+template <int DEG>
+__device__ __forceinline__ double poly_estrin(const double *__restrict__ c, double x) {
+  static_assert(DEG == 11 || DEG == 5, "Boys tables are degree 11 or 5");
+  const double x2 = x * x;
+  if (DEG == 5) {
+    const double p01 = fma(c[1], x, c[0]), p23 = fma(c[3], x, c[2]), p45 = fma(c[5], x, c[4]);
+    return fma(fma(p45, x2, p23), x2, p01);
+  }
+  const double x4 = x2 * x2;
+  const double p01 = fma(c[1], x, c[0]), p23 = fma(c[3], x, c[2]), p45 = fma(c[5], x, c[4]);
+  const double p67 = fma(c[7], x, c[6]), p89 = fma(c[9], x, c[8]), pab = fma(c[11], x, c[10]);
+  const double q0 = fma(p23, x2, p01), q1 = fma(p67, x2, p45), q2 = fma(pab, x2, p89);
+  return fma(fma(q2, x4, q1), x4, q0);
+}
+
 // F_0..F_M(T): table polynomial for F_M below kBoysTmax then downward
 // recursion F_m = (2T F_{m+1} + e^-T)/(2m+1); above it F_0 = sqrt(pi/T)/2
-// and upward recursion F_{m+1} = ((2m+1) F_m - e^-T)/(2T).
-template <int M>
+// and upward recursion F_{m+1} = ((2m+1) F_m - e^-T)/(2T).  DEG 11 is the
+// full-accuracy table (relative error ~1e-16); DEG 5 is the table of the
+// FP32 half of the mixed form (relative error ~2e-8, FP64 arithmetic).
+template <int M, int DEG = kBoysDeg>
 __device__ __forceinline__ void boys_eval(double T, const double *__restrict__ tab, double *F) {
   if (T < kBoysTmax) {
     int i = (int)(T * kBoysPerUnit);
     double x = (T - (i + 0.5) * (1.0 / kBoysPerUnit)) * (2.0 * kBoysPerUnit);
-    const double *c = tab + i * kBoysNcoef;
-    double f = c[kBoysDeg];
-#pragma unroll
-    for (int k = kBoysDeg - 1; k >= 0; --k) f = fma(f, x, c[k]);
-    F[M] = f;
+    F[M] = poly_estrin<DEG>(tab + i * kBoysNcoef, x);
     if (M > 0) {
       double et = exp(-T), t2 = 2.0 * T;
 #pragma unroll
