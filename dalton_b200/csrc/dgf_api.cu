@@ -2,6 +2,7 @@
 // data, Schwarz factors, class-sorted pair lists), the HERFCK-semantics Fock
 // build, and the Boys/spherical tables.
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -179,8 +180,8 @@ static void free_ctx(dgf_ctx *c) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
-  void *ptrs[] = {c->d_pairs, c->d_pp, c->d_boys, c->d_sph, c->d_D, c->d_Ds, c->d_Fh,
-                  c->d_io, c->d_dmax, c->d_cnt, c->d_qoff};
+  void *ptrs[] = {c->d_pairs, c->d_pp,     c->d_boys,   c->d_sph,   c->d_D,     c->d_Ds,    c->d_Fh, c->d_io,
+                  c->d_dmax,  c->d_cnt,    c->d_qoff,   c->d_wmap_i, c->d_wmap_c, c->d_wmeta, c->d_wdims, c->d_gw};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -343,41 +344,238 @@ static JKArgs base_args(dgf_ctx *c) {
   a.pp = c->d_pp;
   a.sph = c->d_sph;
   a.spherical = c->spherical;
-  a.nbf = c->nbf;
-  a.nshell = c->nshell;
-  a.slot_stride = (int64_t)c->nbf * c->nbf;
+  a.nbf = c->nwf;
+  a.nshell = c->nwshell;
+  a.slot_stride = (int64_t)c->nwf * c->nwf;
   return a;
 }
 
-// Schwarz factors: (ab|ab) of every pair with the diag mode of the kernels
-// (GABGEN/GABDRV, DALTON/abacus/her2gab.F:36,1776).
-static int compute_schwarz(dgf_ctx *c) {
-  const int np = (int)c->pairs.size();
+// Schwarz factors: (ab|ab) of every pair of a class-major pair list with the
+// diag mode of the kernels (GABGEN/GABDRV, DALTON/abacus/her2gab.F:36,1776).
+static int schwarz_of(dgf_ctx *c, const PairRec *d_pairs, const PrimPair *d_pp, const int *cls_off,
+                      std::vector<double> &q) {
+  const int np = cls_off[kNumPairClass];
+  q.assign(np, 0.0);
+  if (np == 0) return DGF_OK;
   double *d_q = nullptr;
   DGF_CUDA_CHECK(dev_alloc(&d_q, np));
   for (int X = 0; X < kNumPairClass; ++X) {
-    const int n = c->cls_off[X + 1] - c->cls_off[X];
+    const int n = cls_off[X + 1] - cls_off[X];
     if (!n) continue;
     const int la = (X == 0) ? 0 : (X <= 2) ? 1 : (X <= 5) ? 2 : 3;
     JKArgs a = base_args(c);
-    a.bra = a.ket = c->d_pairs + c->cls_off[X];
+    a.pp = d_pp;
+    a.bra = a.ket = d_pairs + cls_off[X];
     a.nbra = n;
     a.nquartet = n;
     a.same_class = 1;
     a.boys = c->d_boys + (size_t)(2 * (la + (X - la * (la + 1) / 2))) * kBoysTableDoubles;
-    a.diag_out = d_q + c->cls_off[X];
+    a.diag_out = d_q + cls_off[X];
     int st = launch_class(c, X, X, a, c->stream, 2);
     if (st) {
       cudaFree(d_q);
       return st;
     }
   }
-  std::vector<double> q(np);
   cudaError_t e = cudaMemcpyAsync(q.data(), d_q, np * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFree(d_q);
   DGF_CUDA_CHECK(e);
-  for (int i = 0; i < np; ++i) c->pairs[i].Q = q[i];
+  return DGF_OK;
+}
+
+static int compute_schwarz(dgf_ctx *c) {
+  std::vector<double> q;
+  int st = schwarz_of(c, c->d_pairs, c->d_pp, c->cls_off, q);
+  if (st) return st;
+  for (size_t i = 0; i < q.size(); ++i) c->pairs[i].Q = q[i];
+  return DGF_OK;
+}
+
+struct ShellList {
+  const std::vector<int> &l, &atom, &ao, &nprim, &p0;
+  const std::vector<double> &a, &c;
+};
+
+// Shell pairs A >= B (the higher l first) with their primitive pairs, class
+// by class; primitive pairs with mu |AB|^2 > 40 (e^-40 ~ 4e-18) are dropped.
+static void build_pairs(const dgf_ctx *c, const ShellList &sh, int nbfm, std::vector<PairRec> &pairs,
+                        int *cls_off, std::vector<PrimPair> &pp) {
+  const double r2pi52 = std::sqrt(2.0 * std::pow(3.14159265358979323846, 2.5));
+  std::vector<std::vector<PairRec>> bycls(kNumPairClass);
+  pp.clear();
+  pairs.clear();
+  const int nsh = (int)sh.l.size();
+  for (int A = 0; A < nsh; ++A)
+    for (int B = 0; B <= A; ++B) {
+      int sa = A, sb = B;
+      if (sh.l[sb] > sh.l[sa]) std::swap(sa, sb);
+      const int la = sh.l[sa], lb = sh.l[sb];
+      const double *xa = &c->xyz[3 * sh.atom[sa]], *xb = &c->xyz[3 * sh.atom[sb]];
+      const double ab2 = (xa[0] - xb[0]) * (xa[0] - xb[0]) + (xa[1] - xb[1]) * (xa[1] - xb[1]) +
+                         (xa[2] - xb[2]) * (xa[2] - xb[2]);
+      PairRec r;
+      memset(&r, 0, sizeof(r));
+      r.shA = sa;
+      r.shB = sb;
+      r.aoA = sh.ao[sa];
+      r.aoB = sh.ao[sb];
+      r.same = (A == B);
+      r.atA = sh.atom[sa];
+      r.atB = sh.atom[sb];
+      r.nbfm = nbfm;
+      r.dbase = 0;
+      r.pp0 = (int)pp.size();
+      for (int i = 0; i < sh.nprim[sa]; ++i)
+        for (int j = 0; j < sh.nprim[sb]; ++j) {
+          const double ea = sh.a[sh.p0[sa] + i], eb = sh.a[sh.p0[sb] + j];
+          const double p = ea + eb, mu = ea * eb / p;
+          if (mu * ab2 > 40.0) continue;
+          PrimPair q;
+          q.p = p;
+          q.Px = (ea * xa[0] + eb * xb[0]) / p;
+          q.Py = (ea * xa[1] + eb * xb[1]) / p;
+          q.Pz = (ea * xa[2] + eb * xb[2]) / p;
+          q.PAx = q.Px - xa[0];
+          q.PAy = q.Py - xa[1];
+          q.PAz = q.Pz - xa[2];
+          q.PBx = q.Px - xb[0];
+          q.PBy = q.Py - xb[1];
+          q.PBz = q.Pz - xb[2];
+          q.K = sh.c[sh.p0[sa] + i] * sh.c[sh.p0[sb] + j] * std::exp(-mu * ab2) * r2pi52 / p;
+          q.ea = ea;
+          pp.push_back(q);
+        }
+      r.npp = (int)pp.size() - r.pp0;
+      if (r.npp == 0) continue;
+      bycls[pair_class(la, lb)].push_back(r);
+    }
+  cls_off[0] = 0;
+  for (int X = 0; X < kNumPairClass; ++X) {
+    cls_off[X + 1] = cls_off[X] + (int)bycls[X].size();
+    pairs.insert(pairs.end(), bycls[X].begin(), bycls[X].end());
+  }
+}
+
+// Working basis (see dgf_work.h).  A block is a general contraction when
+// some primitive has a nonzero coefficient in two or more of its contracted
+// functions; such a block becomes one single-primitive shell per primitive,
+// scaled by its largest coefficient so that the working functions keep the
+// magnitude of the contracted ones (C entries = coefficient / scale, at most
+// 1 in size).  Other blocks keep one shell per contracted function with its
+// nonzero primitives (C entries 1).  Working functions are numbered block by
+// block, shell by shell, component by component.
+static int build_working_basis(dgf_ctx *c, const dgf_basis *b) {
+  WorkMapHost &wm = c->wmap;
+  std::vector<std::vector<std::pair<int, double>>> rows;
+  int wao = 0;
+  c->w_identity = 1;
+  for (dgf_int ib = 0; ib < b->nblock; ++ib) {
+    const int l = (int)b->block_l[ib], np = (int)b->block_nprim[ib], nc = (int)b->block_ncontr[ib];
+    const int at = (int)b->block_atom[ib], nf = nfun(l, c->spherical);
+    const double *cf = b->coef + b->block_coef_offset[ib];  // column-major (np, nc)
+    const double *ex = b->prim_exp + b->block_prim_offset[ib];
+    bool general = false;
+    for (int i = 0; i < np && !general; ++i) {
+      int used = 0;
+      for (int k = 0; k < nc; ++k) used += (cf[(size_t)k * np + i] != 0.0);
+      general = used >= 2;
+    }
+    if (general) {
+      c->w_identity = 0;
+      for (int i = 0; i < np; ++i) {
+        double scale = 0.0;
+        for (int k = 0; k < nc; ++k) scale = std::max(scale, std::fabs(cf[(size_t)k * np + i]));
+        if (scale == 0.0) continue;
+        c->ws_l.push_back(l);
+        c->ws_atom.push_back(at);
+        c->ws_ao.push_back(wao);
+        c->ws_p0.push_back((int)c->ws_a.size());
+        c->ws_nprim.push_back(1);
+        c->ws_a.push_back(ex[i]);
+        c->ws_c.push_back(scale);
+        for (int m = 0; m < nf; ++m) {
+          std::vector<std::pair<int, double>> r;
+          for (int k = 0; k < nc; ++k) {
+            const double v = cf[(size_t)k * np + i];
+            if (v != 0.0) r.push_back({(int)b->block_ao_offset[ib] + k * nf + m, v / scale});
+          }
+          rows.push_back(std::move(r));
+        }
+        wao += nf;
+      }
+    } else {
+      for (int k = 0; k < nc; ++k) {
+        c->ws_l.push_back(l);
+        c->ws_atom.push_back(at);
+        c->ws_ao.push_back(wao);
+        c->ws_p0.push_back((int)c->ws_a.size());
+        int cnt = 0;
+        for (int i = 0; i < np; ++i) {
+          const double v = cf[(size_t)k * np + i];
+          if (v == 0.0) continue;
+          c->ws_a.push_back(ex[i]);
+          c->ws_c.push_back(v);
+          ++cnt;
+        }
+        c->ws_nprim.push_back(cnt);
+        for (int m = 0; m < nf; ++m) {
+          const int ao = (int)b->block_ao_offset[ib] + k * nf + m;
+          if (ao != wao + m) c->w_identity = 0;
+          rows.push_back({{ao, 1.0}});
+        }
+        wao += nf;
+      }
+    }
+  }
+  c->nwf = wao;
+  c->nwshell = (int)c->ws_l.size();
+  if (c->nwf != (int)rows.size()) DGF_FAIL(DGF_ERR_ARG, "inconsistent working basis");
+  wm = WorkMapHost();
+  wm.wr_off.assign(c->nwf + 1, 0);
+  for (int p = 0; p < c->nwf; ++p) {
+    wm.wr_off[p + 1] = wm.wr_off[p] + (int)rows[p].size();
+    for (const auto &e : rows[p]) {
+      wm.wr_idx.push_back(e.first);
+      wm.wr_c.push_back(e.second);
+    }
+  }
+  // transpose: AO function -> working functions
+  wm.ac_off.assign(c->nbf + 1, 0);
+  for (int mu : wm.wr_idx) ++wm.ac_off[mu + 1];
+  for (int mu = 0; mu < c->nbf; ++mu) wm.ac_off[mu + 1] += wm.ac_off[mu];
+  wm.ac_idx.assign(wm.wr_idx.size(), 0);
+  wm.ac_c.assign(wm.wr_idx.size(), 0.0);
+  std::vector<int> fill(wm.ac_off.begin(), wm.ac_off.end() - 1);
+  for (int p = 0; p < c->nwf; ++p)
+    for (int i = wm.wr_off[p]; i < wm.wr_off[p + 1]; ++i) {
+      const int pos = fill[wm.wr_idx[i]]++;
+      wm.ac_idx[pos] = p;
+      wm.ac_c[pos] = wm.wr_c[i];
+    }
+  return DGF_OK;
+}
+
+static int upload_working_maps(dgf_ctx *c) {
+  const WorkMapHost &wm = c->wmap;
+  std::vector<int> ints;
+  ints.insert(ints.end(), wm.wr_off.begin(), wm.wr_off.end());
+  ints.insert(ints.end(), wm.wr_idx.begin(), wm.wr_idx.end());
+  ints.insert(ints.end(), wm.ac_off.begin(), wm.ac_off.end());
+  ints.insert(ints.end(), wm.ac_idx.begin(), wm.ac_idx.end());
+  std::vector<double> cs(wm.wr_c);
+  cs.insert(cs.end(), wm.ac_c.begin(), wm.ac_c.end());
+  const int64_t meta[4] = {0, (int64_t)c->nwf * c->nwf, 0, (int64_t)c->nbf * c->nbf};
+  const int dims[4] = {c->nwf, c->nbf, 0, 0};
+  if (dev_alloc(&c->d_wmap_i, ints.size()) != cudaSuccess || dev_alloc(&c->d_wmap_c, std::max<size_t>(cs.size(), 1)) != cudaSuccess ||
+      dev_alloc(&c->d_wmeta, 4) != cudaSuccess || dev_alloc(&c->d_wdims, 4) != cudaSuccess) {
+    cudaGetLastError();
+    DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the working-basis maps failed");
+  }
+  DGF_CUDA_CHECK(cudaMemcpy(c->d_wmap_i, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (!cs.empty()) DGF_CUDA_CHECK(cudaMemcpy(c->d_wmap_c, cs.data(), cs.size() * 8, cudaMemcpyHostToDevice));
+  DGF_CUDA_CHECK(cudaMemcpy(c->d_wmeta, meta, sizeof(meta), cudaMemcpyHostToDevice));
+  DGF_CUDA_CHECK(cudaMemcpy(c->d_wdims, dims, sizeof(dims), cudaMemcpyHostToDevice));
   return DGF_OK;
 }
 
@@ -449,61 +647,13 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
   }
   c->nshell = (int)c->sh_l.size();
 
-  // Shell pairs A >= B (the higher l first) with their primitive pairs;
-  // primitive pairs with mu |AB|^2 > 40 (e^-40 ~ 4e-18) are dropped.
-  const double r2pi52 = std::sqrt(2.0 * std::pow(3.14159265358979323846, 2.5));
-  std::vector<std::vector<PairRec>> bycls(kNumPairClass);
-  std::vector<PrimPair> pp;
-  for (int A = 0; A < c->nshell; ++A)
-    for (int B = 0; B <= A; ++B) {
-      int sa = A, sb = B;
-      if (c->sh_l[sb] > c->sh_l[sa]) std::swap(sa, sb);
-      const int la = c->sh_l[sa], lb = c->sh_l[sb];
-      const double *xa = &c->xyz[3 * c->sh_atom[sa]], *xb = &c->xyz[3 * c->sh_atom[sb]];
-      const double ab2 = (xa[0] - xb[0]) * (xa[0] - xb[0]) + (xa[1] - xb[1]) * (xa[1] - xb[1]) +
-                         (xa[2] - xb[2]) * (xa[2] - xb[2]);
-      PairRec r;
-      memset(&r, 0, sizeof(r));
-      r.shA = sa;
-      r.shB = sb;
-      r.aoA = c->sh_ao[sa];
-      r.aoB = c->sh_ao[sb];
-      r.same = (A == B);
-      r.atA = c->sh_atom[sa];
-      r.atB = c->sh_atom[sb];
-      r.nbfm = c->nbf;
-      r.dbase = 0;
-      r.pp0 = (int)pp.size();
-      for (int i = 0; i < c->sh_nprim[sa]; ++i)
-        for (int j = 0; j < c->sh_nprim[sb]; ++j) {
-          const double ea = c->sh_a[c->sh_p0[sa] + i], eb = c->sh_a[c->sh_p0[sb] + j];
-          const double p = ea + eb, mu = ea * eb / p;
-          if (mu * ab2 > 40.0) continue;
-          PrimPair q;
-          q.p = p;
-          q.Px = (ea * xa[0] + eb * xb[0]) / p;
-          q.Py = (ea * xa[1] + eb * xb[1]) / p;
-          q.Pz = (ea * xa[2] + eb * xb[2]) / p;
-          q.PAx = q.Px - xa[0];
-          q.PAy = q.Py - xa[1];
-          q.PAz = q.Pz - xa[2];
-          q.PBx = q.Px - xb[0];
-          q.PBy = q.Py - xb[1];
-          q.PBz = q.Pz - xb[2];
-          q.K = c->sh_c[c->sh_p0[sa] + i] * c->sh_c[c->sh_p0[sb] + j] * std::exp(-mu * ab2) * r2pi52 / p;
-          q.ea = ea;
-          pp.push_back(q);
-        }
-      r.npp = (int)pp.size() - r.pp0;
-      if (r.npp == 0) continue;
-      bycls[pair_class(la, lb)].push_back(r);
-    }
-  c->pp.swap(pp);
-  c->cls_off[0] = 0;
-  for (int X = 0; X < kNumPairClass; ++X) {
-    c->cls_off[X + 1] = c->cls_off[X] + (int)bycls[X].size();
-    c->pairs.insert(c->pairs.end(), bycls[X].begin(), bycls[X].end());
-  }
+  // Two-electron working basis and its map to the AO basis.
+  int st_wb = build_working_basis(c.get(), b);
+  if (st_wb) return st_wb;
+
+  // Working-basis shell pairs with their primitive pairs.
+  build_pairs(c.get(), ShellList{c->ws_l, c->ws_atom, c->ws_ao, c->ws_nprim, c->ws_p0, c->ws_a, c->ws_c}, c->nwf,
+              c->pairs, c->cls_off, c->pp);
 
   DGF_CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   DGF_CUDA_CHECK(cudaEventCreate(&c->ev0));
@@ -523,7 +673,9 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
   DGF_CUDA_CHECK(cudaMemcpy(c->d_pp, c->pp.data(), c->pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice));
   DGF_CUDA_CHECK(
       cudaMemcpy(c->d_pairs, c->pairs.data(), c->pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice));
-  int st = compute_schwarz(c.get());
+  int st = upload_working_maps(c.get());
+  if (st) return st;
+  st = compute_schwarz(c.get());
   if (st) return st;
   // Sort each class by (primitive-count bucket, Schwarz factor descending)
   // and record the bucket boundaries, then re-upload.
@@ -553,6 +705,60 @@ extern "C" int dgf_info(const dgf_ctx *c, dgf_int *nbf, dgf_int *natom, dgf_int 
   if (nbf) *nbf = c->nbf;
   if (natom) *natom = c->natom;
   if (nshell) *nshell = c->nshell;
+  return DGF_OK;
+}
+
+// Significant contracted shell quartets of the AO basis (one shell per
+// contracted function, canonical A >= B, C >= D, AB >= CD, Q_AB Q_CD >= thrs):
+// the size of a Fock build in the units Dalton-style codes count, independent
+// of the working basis the kernels use.  Builds the AO pair list and its
+// Schwarz factors once per call; not meant for a hot loop.
+extern "C" int dgf_count_ao_quartets(dgf_ctx *c, double thrs, dgf_int *count) {
+  if (!c || !count) DGF_FAIL(DGF_ERR_ARG, "NULL argument");
+  if (!(thrs >= 0.0)) DGF_FAIL(DGF_ERR_ARG, "thrs must be >= 0");
+  DeviceGuard g(c->device);
+  std::vector<PairRec> pairs;
+  std::vector<PrimPair> pp;
+  int cls_off[kNumPairClass + 1];
+  build_pairs(c, ShellList{c->sh_l, c->sh_atom, c->sh_ao, c->sh_nprim, c->sh_p0, c->sh_a, c->sh_c}, c->nbf, pairs,
+              cls_off, pp);
+  PairRec *d_pairs = nullptr;
+  PrimPair *d_pp = nullptr;
+  if (dev_alloc(&d_pairs, std::max<size_t>(pairs.size(), 1)) != cudaSuccess ||
+      dev_alloc(&d_pp, std::max<size_t>(pp.size(), 1)) != cudaSuccess) {
+    cudaGetLastError();
+    if (d_pairs) cudaFree(d_pairs);
+    DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the AO pair list failed");
+  }
+  cudaError_t e = cudaMemcpy(d_pairs, pairs.data(), pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_pp, pp.data(), pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice);
+  std::vector<double> q;
+  int st = (e == cudaSuccess) ? schwarz_of(c, d_pairs, d_pp, cls_off, q) : DGF_ERR_CUDA;
+  cudaFree(d_pairs);
+  cudaFree(d_pp);
+  if (e != cudaSuccess) DGF_FAIL(DGF_ERR_CUDA, cudaGetErrorString(e));
+  if (st) return st;
+  int64_t total = 0;
+  for (int X = 0; X < kNumPairClass; ++X) {
+    std::vector<double> qb(q.begin() + cls_off[X], q.begin() + cls_off[X + 1]);
+    std::sort(qb.begin(), qb.end(), std::greater<double>());
+    for (int Y = 0; Y <= X; ++Y) {
+      std::vector<double> qk(q.begin() + cls_off[Y], q.begin() + cls_off[Y + 1]);
+      std::sort(qk.begin(), qk.end(), std::greater<double>());
+      for (size_t i = 0; i < qb.size(); ++i) {
+        size_t lo = 0, hi = qk.size();  // kets with qb * Q >= thrs form a prefix
+        while (lo < hi) {
+          const size_t mid = (lo + hi) >> 1;
+          if (qb[i] * qk[mid] >= thrs)
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        total += (int64_t)((X == Y) ? std::min(lo, i + 1) : lo);
+      }
+    }
+  }
+  *count = total;
   return DGF_OK;
 }
 
@@ -619,7 +825,7 @@ int dgf_plan_for(dgf_ctx *c, double thrs) { return build_plan(c, thrs); }
 
 static int ensure_slots(dgf_ctx *c, int nslot) {
   if (nslot <= c->cap_slots) return DGF_OK;
-  const size_t n2 = (size_t)c->nbf * c->nbf;
+  const size_t n2 = (size_t)c->nwf * c->nwf;
   for (double **p : {&c->d_D, &c->d_Ds, &c->d_Fh}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
@@ -632,36 +838,12 @@ static int ensure_slots(dgf_ctx *c, int nslot) {
   }
   c->cap_slots = nslot;
   if (!c->d_dmax) {
-    if (dev_alloc(&c->d_dmax, (size_t)c->nshell * c->nshell) != cudaSuccess) {
+    if (dev_alloc(&c->d_dmax, (size_t)c->nwshell * c->nwshell) != cudaSuccess) {
       cudaGetLastError();
       DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the density bound failed");
     }
   }
   return DGF_OK;
-}
-
-// Slot preparation: slot s takes density `src` with op 0 = copy, 1 = transpose,
-// 2 = symmetric part, 3 = antisymmetric part; Ds = D_slot + D_slot^T.
-__global__ void prep_slot_kernel(const double *__restrict__ Din, double *__restrict__ D, double *__restrict__ Ds,
-                                 int n, int op) {
-  const int64_t n2 = (int64_t)n * n;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n2; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t p = e / n, q = e - p * n;
-    const double a = Din[e], t = Din[q * n + p];
-    double v = (op == 0) ? a : (op == 1) ? t : (op == 2) ? 0.5 * (a + t) : 0.5 * (a - t);
-    D[e] = v;
-    Ds[e] = (op == 3) ? 0.0 : a + t;
-  }
-}
-
-// Output: F = Fh1 + sign * Fh2^T.
-__global__ void combine_kernel(const double *__restrict__ F1, const double *__restrict__ F2, double *__restrict__ F,
-                               int n, double sign) {
-  const int64_t n2 = (int64_t)n * n;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n2; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t p = e / n, q = e - p * n;
-    F[e] = F1[e] + sign * F2[q * n + p];
-  }
 }
 
 // Block maxima of |D| per shell pair over all slots (MKDRAO, her2gab.F:1213).
@@ -696,8 +878,10 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   if (!(o.thrs >= 0.0)) DGF_FAIL(DGF_ERR_ARG, "thrs must be >= 0");
   if (o.shard_count <= 0) o.shard_count = 1;
   if (o.shard_index < 0 || o.shard_index >= o.shard_count) DGF_FAIL(DGF_ERR_ARG, "shard_index out of range");
-  const int N = c->nbf;
+  const int N = c->nwf;                            // working basis
   const size_t n2 = (size_t)N * N;
+  const size_t n2ao = (size_t)c->nbf * c->nbf;     // AO-basis inputs and outputs
+  const WorkMaps wmaps = ctx_maps(c);
   // Decode IFCTYP into density slots and output combinations.
   std::vector<SlotSpec> slots;
   struct OutSpec {
@@ -749,30 +933,30 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   int64_t launches = 0, total_q = 0, nlaunch_class = 0;
   for (const ClassPlan &cp : c->plan)
     total_q += cp.nquartet * (o.shard_index + 1) / o.shard_count - cp.nquartet * o.shard_index / o.shard_count;
-  const int eb = 256, eg = (int)std::min<size_t>((n2 + eb - 1) / eb, (size_t)c->nsm * 8);
   // Zero outputs that have no contributions.
   for (int k = 0; k < ndmat; ++k)
-    if (outs[k].zero) DGF_CUDA_CHECK(cudaMemsetAsync(fmat_dev + (size_t)k * n2, 0, n2 * 8, st));
-  std::vector<int> sh_nf(c->nshell);
+    if (outs[k].zero) DGF_CUDA_CHECK(cudaMemsetAsync(fmat_dev + (size_t)k * n2ao, 0, n2ao * 8, st));
+  const int nws = c->nwshell;
+  std::vector<int> sh_nf(nws);
   int *d_shinfo = nullptr;
   if (need_dmax) {
-    for (int s = 0; s < c->nshell; ++s) sh_nf[s] = nfun(c->sh_l[s], c->spherical);
-    DGF_CUDA_CHECK(dev_alloc(&d_shinfo, 2 * (size_t)c->nshell));
-    DGF_CUDA_CHECK(cudaMemcpyAsync(d_shinfo, c->sh_ao.data(), c->nshell * 4, cudaMemcpyHostToDevice, st));
-    DGF_CUDA_CHECK(cudaMemcpyAsync(d_shinfo + c->nshell, sh_nf.data(), c->nshell * 4, cudaMemcpyHostToDevice, st));
+    for (int s = 0; s < nws; ++s) sh_nf[s] = nfun(c->ws_l[s], c->spherical);
+    DGF_CUDA_CHECK(dev_alloc(&d_shinfo, 2 * (size_t)nws));
+    DGF_CUDA_CHECK(cudaMemcpyAsync(d_shinfo, c->ws_ao.data(), nws * 4, cudaMemcpyHostToDevice, st));
+    DGF_CUDA_CHECK(cudaMemcpyAsync(d_shinfo + nws, sh_nf.data(), nws * 4, cudaMemcpyHostToDevice, st));
   }
   for (int s0 = 0; s0 < nslot_total; s0 += chunk) {
     const int ns = std::min(chunk, nslot_total - s0);
     for (int s = 0; s < ns; ++s) {
       const SlotSpec &sp = slots[s0 + s];
-      prep_slot_kernel<<<eg, eb, 0, st>>>(dmat_dev + (size_t)sp.src * n2, c->d_D + s * n2, c->d_Ds + s * n2, N,
-                                          sp.op);
+      launch_work_prep(wmaps, dmat_dev + (size_t)sp.src * n2ao, c->d_D + s * n2, c->d_Ds + s * n2, sp.op,
+                       (int64_t)n2, c->nsm, st);
       ++launches;
     }
     DGF_CUDA_CHECK(cudaMemsetAsync(c->d_Fh, 0, ns * n2 * 8, st));
     if (need_dmax) {
-      dmax_kernel<<<std::max(1, std::min(c->nshell * c->nshell / 128 + 1, c->nsm * 8)), 128, 0, st>>>(
-          c->d_D, ns, N, d_shinfo, d_shinfo + c->nshell, c->nshell, c->d_dmax);
+      dmax_kernel<<<std::max(1, std::min(nws * nws / 128 + 1, c->nsm * 8)), 128, 0, st>>>(
+          c->d_D, ns, N, d_shinfo, d_shinfo + nws, nws, c->d_dmax);
       ++launches;
     }
     JKArgs a = base_args(c);
@@ -823,8 +1007,8 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     for (int k = 0; k < ndmat; ++k) {
       const OutSpec &os = outs[k];
       if (os.zero || os.s1 < s0 || os.s1 >= s0 + ns) continue;
-      combine_kernel<<<eg, eb, 0, st>>>(c->d_Fh + (os.s1 - s0) * n2, c->d_Fh + (os.s2 - s0) * n2,
-                                        fmat_dev + (size_t)k * n2, N, os.sign);
+      launch_work_combine(wmaps, c->d_Fh + (os.s1 - s0) * n2, c->d_Fh + (os.s2 - s0) * n2,
+                          fmat_dev + (size_t)k * n2ao, os.sign, (int64_t)n2ao, c->nsm, st);
       ++launches;
     }
   }
@@ -917,6 +1101,14 @@ extern "C" const char *dgf_strerror(int s) {
 
 extern "C" const char *dgf_last_error(void) { return dgf::g_last_error.c_str(); }
 
+// Copy the per-class kernel choices of one context to another (contexts of
+// similar molecules share a tuning run).
+extern "C" int dgf_copy_tuning(dgf_ctx *dst, const dgf_ctx *src) {
+  if (!dst || !src) DGF_FAIL(DGF_ERR_ARG, "NULL context");
+  memcpy(dst->choice, src->choice, sizeof(dst->choice));
+  return DGF_OK;
+}
+
 // Per-class autotuner: times every candidate kernel of every class pair of
 // the current plan on the given density (team kernel and each thread-kernel
 // chunk variant, FP64 and FP32) with CUDA events and keeps the fastest.
@@ -932,9 +1124,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
   if (r) return r;
   r = ensure_slots(c, 1);
   if (r) return r;
-  const size_t n2 = (size_t)c->nbf * c->nbf;
-  const int eb = 256, eg = (int)std::min<size_t>((n2 + eb - 1) / eb, (size_t)c->nsm * 8);
-  prep_slot_kernel<<<eg, eb, 0, st>>>(dmat_device, c->d_D, c->d_Ds, c->nbf, 2);
+  launch_work_prep(ctx_maps(c), dmat_device, c->d_D, c->d_Ds, 2, (int64_t)c->nwf * c->nwf, c->nsm, st);
   DGF_CUDA_CHECK(cudaGetLastError());
   cudaEvent_t e0, e1;
   DGF_CUDA_CHECK(cudaEventCreate(&e0));

@@ -5,8 +5,10 @@
 // Every molecule keeps its own canonical quartet list (no cross-molecule
 // quartets): the merged pair list of a class is the concatenation of the
 // molecules' Schwarz-sorted lists, each pair record carries its molecule's
-// offset and size in the packed D/F storage, and the plan stores, per bra
-// pair, the first ket of its molecule in the merged ket list.
+// offset and size in the packed working-basis D/F storage, and the plan
+// stores, per bra pair, the first ket of its molecule in the merged ket
+// list.  The packed AO-basis matrices of the caller are mapped to and from
+// the packed working-basis ones by one transform launch each.
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -26,17 +28,21 @@ struct BatchPlan {
 
 struct dgf_batch {
   int device = 0, nmol = 0, spherical = 1, nsm = 148;
-  std::vector<int64_t> offsets;  // nmol+1 packed offsets
-  std::vector<int> nbf;
-  int64_t total = 0;
+  std::vector<int64_t> offsets;   // nmol+1 packed AO-matrix offsets (the caller's layout)
+  std::vector<int64_t> woffsets;  // nmol+1 packed working-matrix offsets
+  std::vector<int> nbf, nwf;
+  int64_t total = 0, total_w = 0;
   std::vector<PairRec> pairs;
   int cls_off[kNumPairClass + 1] = {0};
   std::vector<int> mol_cls_off;  // [X * nmol + m]: start of molecule m's class-X pairs in the merged list
   PairRec *d_pairs = nullptr;
   PrimPair *d_pp = nullptr;
   double *d_boys = nullptr, *d_sph = nullptr;
-  int64_t *d_offsets = nullptr;
-  int *d_nbf = nullptr;
+  int64_t *d_offsets = nullptr;  // AO offsets | working offsets
+  int *d_dims = nullptr;          // nwf | nbf | working base | AO base, nmol each
+  int *d_wmap_i = nullptr;
+  double *d_wmap_c = nullptr;
+  WorkMaps maps;
   double *d_D = nullptr, *d_Ds = nullptr, *d_Fh = nullptr;
   unsigned long long *d_cnt = nullptr;
   double plan_thrs = -1.0;
@@ -52,6 +58,7 @@ struct dgf_batch {
   double g_thrs = -1.0, g_hfx = 0.0;
   cudaStream_t g_stream = nullptr;
   int64_t launches = 0;
+  int choice[kNumPairClass][kNumPairClass] = {};  // FP64 kernel per class pair (from the largest context)
 };
 
 static void batch_free(dgf_batch *b) {
@@ -59,8 +66,8 @@ static void batch_free(dgf_batch *b) {
   DeviceGuard g(b->device);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  void *ptrs[] = {b->d_pairs, b->d_pp, b->d_boys, b->d_sph, b->d_offsets, b->d_nbf, b->d_D, b->d_Ds, b->d_Fh,
-                  b->d_cnt, b->d_qoff, b->d_kbase};
+  void *ptrs[] = {b->d_pairs, b->d_pp, b->d_boys, b->d_sph, b->d_offsets, b->d_dims, b->d_wmap_i, b->d_wmap_c,
+                  b->d_D,     b->d_Ds, b->d_Fh,   b->d_cnt, b->d_qoff,    b->d_kbase};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -94,11 +101,47 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
   b->nsm = ctxs[0]->nsm;
   DeviceGuard g(dev);
   b->offsets.assign(nmol + 1, 0);
+  b->woffsets.assign(nmol + 1, 0);
   for (dgf_int m = 0; m < nmol; ++m) {
     b->nbf.push_back(ctxs[m]->nbf);
+    b->nwf.push_back(ctxs[m]->nwf);
     b->offsets[m + 1] = b->offsets[m] + (int64_t)ctxs[m]->nbf * ctxs[m]->nbf;
+    b->woffsets[m + 1] = b->woffsets[m] + (int64_t)ctxs[m]->nwf * ctxs[m]->nwf;
   }
   b->total = b->offsets[nmol];
+  b->total_w = b->woffsets[nmol];
+  dgf_int big = 0;
+  for (dgf_int m = 1; m < nmol; ++m)
+    if (ctxs[m]->nbf > ctxs[big]->nbf) big = m;
+  for (int X = 0; X < kNumPairClass; ++X)
+    for (int Y = 0; Y < kNumPairClass; ++Y) b->choice[X][Y] = ctxs[big]->choice[X][Y][0];
+  // Concatenated AO <-> working maps (offsets made global, indices stay local).
+  std::vector<int> wr_off{0}, wr_idx, ac_off{0}, ac_idx, wbase, abase;
+  std::vector<double> wr_c, ac_c;
+  for (dgf_int m = 0; m < nmol; ++m) {
+    const WorkMapHost &wm = ctxs[m]->wmap;
+    wbase.push_back((int)wr_off.size() - 1);
+    abase.push_back((int)ac_off.size() - 1);
+    const int r0 = (int)wr_idx.size(), c0 = (int)ac_idx.size();
+    for (int p = 0; p < ctxs[m]->nwf; ++p) wr_off.push_back(r0 + wm.wr_off[p + 1]);
+    for (int mu = 0; mu < ctxs[m]->nbf; ++mu) ac_off.push_back(c0 + wm.ac_off[mu + 1]);
+    wr_idx.insert(wr_idx.end(), wm.wr_idx.begin(), wm.wr_idx.end());
+    wr_c.insert(wr_c.end(), wm.wr_c.begin(), wm.wr_c.end());
+    ac_idx.insert(ac_idx.end(), wm.ac_idx.begin(), wm.ac_idx.end());
+    ac_c.insert(ac_c.end(), wm.ac_c.begin(), wm.ac_c.end());
+  }
+  std::vector<int> ints(wr_off);
+  ints.insert(ints.end(), wr_idx.begin(), wr_idx.end());
+  ints.insert(ints.end(), ac_off.begin(), ac_off.end());
+  ints.insert(ints.end(), ac_idx.begin(), ac_idx.end());
+  std::vector<double> cs(wr_c);
+  cs.insert(cs.end(), ac_c.begin(), ac_c.end());
+  std::vector<int> dims(b->nwf);
+  dims.insert(dims.end(), b->nbf.begin(), b->nbf.end());
+  dims.insert(dims.end(), wbase.begin(), wbase.end());
+  dims.insert(dims.end(), abase.begin(), abase.end());
+  std::vector<int64_t> offs(b->offsets);
+  offs.insert(offs.end(), b->woffsets.begin(), b->woffsets.end());
   std::vector<PrimPair> pp;
   std::vector<int64_t> pp_off(nmol);
   for (dgf_int m = 0; m < nmol; ++m) {
@@ -122,8 +165,8 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
       for (const PairRec &src : lst) {
         PairRec r = src;
         r.pp0 += (int)pp_off[m];
-        r.nbfm = c->nbf;
-        r.dbase = b->offsets[m];
+        r.nbfm = c->nwf;
+        r.dbase = b->woffsets[m];
         b->pairs.push_back(r);
       }
     }
@@ -138,11 +181,13 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
   alloc((void **)&b->d_pp, pp.size() * sizeof(PrimPair));
   alloc((void **)&b->d_boys, n_boys * 8);
   alloc((void **)&b->d_sph, kSphTableDoubles * 8);
-  alloc((void **)&b->d_offsets, (nmol + 1) * 8);
-  alloc((void **)&b->d_nbf, nmol * 4);
-  alloc((void **)&b->d_D, b->total * 8);
-  alloc((void **)&b->d_Ds, b->total * 8);
-  alloc((void **)&b->d_Fh, b->total * 8);
+  alloc((void **)&b->d_offsets, offs.size() * 8);
+  alloc((void **)&b->d_dims, dims.size() * 4);
+  alloc((void **)&b->d_wmap_i, ints.size() * 4);
+  alloc((void **)&b->d_wmap_c, cs.size() * 8);
+  alloc((void **)&b->d_D, b->total_w * 8);
+  alloc((void **)&b->d_Ds, b->total_w * 8);
+  alloc((void **)&b->d_Fh, b->total_w * 8);
   alloc((void **)&b->d_cnt, 4 * kCounterSlots * 8);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -153,8 +198,10 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
   if (e == cudaSuccess) e = cudaMemcpy(b->d_pp, pp.data(), pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_boys, ctxs[0]->d_boys, n_boys * 8, cudaMemcpyDeviceToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_sph, ctxs[0]->d_sph, kSphTableDoubles * 8, cudaMemcpyDeviceToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(b->d_offsets, b->offsets.data(), (nmol + 1) * 8, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(b->d_nbf, b->nbf.data(), nmol * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_offsets, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_dims, dims.data(), dims.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_wmap_i, ints.data(), ints.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !cs.empty()) e = cudaMemcpy(b->d_wmap_c, cs.data(), cs.size() * 8, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
@@ -163,6 +210,22 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
     batch_free(b);
     BFAIL(DGF_ERR_CUDA, msg);
   }
+  WorkMaps &mp = b->maps;
+  const int nm = (int)nmol;
+  const size_t nr = wr_idx.size();
+  mp.nmol = nm;
+  mp.a_elem = b->d_offsets;
+  mp.w_elem = b->d_offsets + (nm + 1);
+  mp.nw = b->d_dims;
+  mp.na = b->d_dims + nm;
+  mp.wf_base = b->d_dims + 2 * nm;
+  mp.af_base = b->d_dims + 3 * nm;
+  mp.wr_off = b->d_wmap_i;
+  mp.wr_idx = b->d_wmap_i + wr_off.size();
+  mp.ac_off = b->d_wmap_i + wr_off.size() + nr;
+  mp.ac_idx = b->d_wmap_i + wr_off.size() + nr + ac_off.size();
+  mp.wr_c = b->d_wmap_c;
+  mp.ac_c = b->d_wmap_c + nr;
   *out = b;
   return DGF_OK;
 }
@@ -241,60 +304,18 @@ static int batch_plan(dgf_batch *b, double thrs) {
   return DGF_OK;
 }
 
-__device__ __forceinline__ int mol_of(const int64_t *__restrict__ off, int nmol, int64_t e) {
-  int lo = 0, hi = nmol;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (off[mid] <= e)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
-// Symmetric part of every packed density (IFCTYP 13): D = (D + D^T)/2, Ds = 2 D.
-__global__ void batch_prep_kernel(const double *__restrict__ Din, double *__restrict__ D, double *__restrict__ Ds,
-                                  const int64_t *__restrict__ off, const int *__restrict__ nbf, int nmol,
-                                  int64_t total) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int m = mol_of(off, nmol, e);
-    const int64_t base = off[m], loc = e - base;
-    const int n = nbf[m];
-    const int64_t p = loc / n, q = loc - p * n;
-    const double v = 0.5 * (Din[e] + Din[base + q * n + p]);
-    D[e] = v;
-    Ds[e] = 2.0 * v;
-  }
-}
-
-// F = Fh + Fh^T per packed block.
-__global__ void batch_combine_kernel(const double *__restrict__ Fh, double *__restrict__ F,
-                                     const int64_t *__restrict__ off, const int *__restrict__ nbf, int nmol,
-                                     int64_t total) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int m = mol_of(off, nmol, e);
-    const int64_t base = off[m], loc = e - base;
-    const int n = nbf[m];
-    const int64_t p = loc / n, q = loc - p * n;
-    F[e] = Fh[e] + Fh[base + q * n + p];
-  }
-}
-
 static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double hfx, cudaStream_t st) {
-  const int eb = 256;
-  const int eg = (int)std::max<int64_t>(1, std::min<int64_t>((b->total + eb - 1) / eb, (int64_t)b->nsm * 8));
   int64_t launches = 0;
-  batch_prep_kernel<<<eg, eb, 0, st>>>(din, b->d_D, b->d_Ds, b->d_offsets, b->d_nbf, b->nmol, b->total);
+  launch_work_prep(b->maps, din, b->d_D, b->d_Ds, 2, b->total_w, b->nsm, st);  // symmetric part, IFCTYP 13
   ++launches;
-  if (cudaMemsetAsync(b->d_Fh, 0, b->total * 8, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "memset failed");
+  if (cudaMemsetAsync(b->d_Fh, 0, b->total_w * 8, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "memset failed");
   JKArgs a;
   memset(&a, 0, sizeof(a));
   a.pp = b->d_pp;
   a.sph = b->d_sph;
   a.spherical = b->spherical;
   a.nslot = 1;
-  a.slot_stride = b->total;
+  a.slot_stride = b->total_w;
   a.D = b->d_D;
   a.Ds = b->d_Ds;
   a.Fh = b->d_Fh;
@@ -317,14 +338,16 @@ static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double h
     const int lc = (bp.Y == 0) ? 0 : (bp.Y <= 2) ? 1 : (bp.Y <= 5) ? 2 : 3;
     const int ld = bp.Y - lc * (lc + 1) / 2;
     a.boys = b->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-    const ClassKernel &k = jk_kernel(bp.X, bp.Y, 0);
+    const ClassKernel *kp = &jk_kernel_variant(bp.X, bp.Y, 0, b->choice[bp.X][bp.Y]);
+    if (!kp->launch) kp = &jk_kernel(bp.X, bp.Y, 0);
+    const ClassKernel &k = *kp;
     const int64_t per_block = (k.smem == 0) ? k.block : 1;
     const int grid = (int)std::max<int64_t>(
         1, std::min<int64_t>((bp.nquartet + per_block - 1) / per_block, (int64_t)b->nsm * 16));
     k.launch(a, grid, k.block, k.smem, st);
     ++launches;
   }
-  batch_combine_kernel<<<eg, eb, 0, st>>>(b->d_Fh, fout, b->d_offsets, b->d_nbf, b->nmol, b->total);
+  launch_work_combine(b->maps, b->d_Fh, b->d_Fh, fout, 1.0, b->total, b->nsm, st);  // F = C^T (Fh + Fh^T) C
   ++launches;
   if (cudaGetLastError() != cudaSuccess) BFAIL(DGF_ERR_CUDA, "launch failed in the batched build");
   b->launches = launches;
@@ -340,7 +363,7 @@ extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, do
   if (opt) o = *opt;
   if (o.ifthrs < 20 || o.mixed_cutoff > 0.0 || o.shard_count > 1)
     BFAIL(DGF_ERR_UNSUPPORTED, "batched builds take the FP64 Schwarz-screened form only");
-  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  cudaStream_t st = (cudaStream_t)stream;  // NULL: the legacy default stream, as in dgf_fock_device
   int r = batch_plan(b, o.thrs);
   if (r) return r;
   if (cudaMemsetAsync(b->d_cnt, 0, 4 * kCounterSlots * 8, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "memset failed");

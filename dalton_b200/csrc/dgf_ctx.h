@@ -4,6 +4,7 @@
 
 #include "../../include/dgfock.h"
 #include "dgf_internal.h"
+#include "dgf_work.h"
 
 #define DGF_CUDA_CHECK(expr)                                                   \
   do {                                                                         \
@@ -24,11 +25,37 @@ struct ClassPlan {
   int64_t nquartet;
 };
 
+// Map between the AO basis (Dalton's contracted functions) and the
+// two-electron working basis, as sparse rows: wr_* gives, for every working
+// function, the AO functions it contributes to with the contraction
+// coefficient (D_w = C D C^T); ac_* gives, for every AO function, the working
+// functions it is made of (F = C^T F_w C).  Device copies in one allocation.
+struct WorkMapHost {
+  std::vector<int> wr_off, wr_idx, ac_off, ac_idx;
+  std::vector<double> wr_c, ac_c;
+};
+
 struct dgf_ctx {
   int device = 0, nbf = 0, natom = 0, nshell = 0, spherical = 1, maxl = 0, nsm = 148;
   std::vector<double> xyz, charge;
+  // AO shells: one per contracted function of a Dalton block (one-electron
+  // integrals and gradients work on these)
   std::vector<int> sh_l, sh_atom, sh_ao, sh_nprim, sh_p0;
   std::vector<double> sh_a, sh_c;
+  // Two-electron working basis: a block whose contracted functions share
+  // primitives (a general contraction) is resolved into one shell per
+  // primitive; every other block keeps one shell per contracted function.
+  // nwf functions in nwshell shells; w_identity when no block was resolved
+  // (the working basis is then the AO basis, function for function).
+  int nwf = 0, nwshell = 0, w_identity = 1;
+  std::vector<int> ws_l, ws_atom, ws_ao, ws_nprim, ws_p0;
+  std::vector<double> ws_a, ws_c;
+  WorkMapHost wmap;
+  int *d_wmap_i = nullptr;      // wr_off | wr_idx | ac_off | ac_idx
+  double *d_wmap_c = nullptr;   // wr_c | ac_c
+  int64_t *d_wmeta = nullptr;   // {0, nwf^2} {0, nbf^2} element offsets of the single-molecule form
+  int *d_wdims = nullptr;       // {nwf, nbf, 0, 0}
+  double *d_gw = nullptr;       // working-basis densities of the two-electron gradient (2 nwf^2)
   std::vector<dgf::PairRec> pairs;  // class-major, Schwarz-descending inside a class
   int cls_off[dgf::kNumPairClass + 1] = {0};
   // per class: bucket boundaries (relative to the class start), pairs sorted by (bucket, -Q)
@@ -58,6 +85,26 @@ struct dgf_ctx {
   std::vector<dgf_class_time> prof;
 };
 
+
+// The single-molecule form of the AO <-> working-basis maps of a context.
+inline dgf::WorkMaps ctx_maps(const dgf_ctx *c) {
+  dgf::WorkMaps m;
+  const size_t nr = c->wmap.wr_idx.size();
+  m.nmol = 1;
+  m.w_elem = c->d_wmeta;
+  m.a_elem = c->d_wmeta + 2;
+  m.nw = c->d_wdims;
+  m.na = c->d_wdims + 1;
+  m.wf_base = c->d_wdims + 2;
+  m.af_base = c->d_wdims + 3;
+  m.wr_off = c->d_wmap_i;
+  m.wr_idx = c->d_wmap_i + (c->nwf + 1);
+  m.ac_off = c->d_wmap_i + (c->nwf + 1) + nr;
+  m.ac_idx = c->d_wmap_i + (c->nwf + 1) + nr + (c->nbf + 1);
+  m.wr_c = c->d_wmap_c;
+  m.ac_c = c->d_wmap_c + nr;
+  return m;
+}
 
 struct DeviceGuard {
   int prev = -1;

@@ -290,12 +290,29 @@ static int grad_impl(dgf_ctx *c, const double *d1, const double *d2, double hfx,
     dgf::set_error(__FILE__, __LINE__, cudaGetErrorString(e));
     return DGF_ERR_CUDA;
   }
+  // The densities in the working basis (D_w = C D C^T; the derivative
+  // integrals do not act on the contraction coefficients).
+  const size_t n2w = (size_t)c->nwf * c->nwf;
+  if (!c->d_gw) {
+    if (cudaMalloc(&c->d_gw, 2 * n2w * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      c->d_gw = nullptr;
+      dgf::set_error(__FILE__, __LINE__, "device allocation of the working-basis densities failed");
+      return DGF_ERR_NOMEM;
+    }
+  }
+  const WorkMaps maps = ctx_maps(c);
+  const bool same = (d2 == d1);
+  launch_work_prep(maps, d1, c->d_gw, nullptr, 0, (int64_t)n2w, c->nsm, st);
+  if (!same) launch_work_prep(maps, d2, c->d_gw + n2w, nullptr, 0, (int64_t)n2w, c->nsm, st);
+  d1 = c->d_gw;
+  d2 = same ? c->d_gw : c->d_gw + n2w;
   JKArgs a;
   memset(&a, 0, sizeof(a));
   a.pp = c->d_pp;
   a.sph = c->d_sph;
   a.spherical = c->spherical;
-  a.nbf = c->nbf;
+  a.nbf = c->nwf;
   a.G1 = d1;
   a.G2 = d2;
   a.grad = grad;

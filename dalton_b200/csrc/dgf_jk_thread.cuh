@@ -276,16 +276,14 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
         };
         if constexpr (L <= 2) {
           // two independent primitive quartets per iteration for latency hiding
-          for (int j = 0; j < kt.npp; j += 2) {
+          int j = 0;
+          for (; j + 1 < kt.npp; j += 2) {
             const PrimPair P2a = a.pp[kt.pp0 + j];
-            PrimPair P2b = P2a;
-            if (j + 1 < kt.npp)
-              P2b = a.pp[kt.pp0 + j + 1];
-            else
-              P2b.K = 0.0;
+            const PrimPair P2b = a.pp[kt.pp0 + j + 1];
             ket_prim(P2a);
             ket_prim(P2b);
           }
+          if (j < kt.npp) ket_prim(a.pp[kt.pp0 + j]);
         } else {
           PrimPair nxt = a.pp[kt.pp0];
           for (int j = 0; j < kt.npp; ++j) {

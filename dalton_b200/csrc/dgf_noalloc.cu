@@ -7,11 +7,13 @@
 // own; or a time-critical loop that cannot afford the implicit
 // synchronisation of cudaMalloc/cudaFree.  dgf_fock_device_noalloc serves
 // them: it runs the same quartet-class kernels as dgf_fock_device, but its
-// scratch (the symmetrised density, D + D^T and the half Fock accumulator)
-// lives in one file-scope device array of fixed size that every GPU which
-// loads this library holds until the process exits.
+// scratch (the symmetrised density, D + D^T and the half Fock accumulator,
+// all in the two-electron working basis) lives in one file-scope device
+// array of fixed size that every GPU which loads this library holds until
+// the process exits.
 //
-// Limits and sharing: at most kNoAllocMaxN basis functions; IFCTYP 13
+// Limits and sharing: at most kNoAllocMaxN basis functions and
+// kNoAllocMaxW working functions; IFCTYP 13
 // (J - hfxfac/2 K of one symmetric density), all-FP64, Schwarz screening
 // only; the context's quartet plan for `thrs` must already exist (any
 // earlier dgf_fock, dgf_fock_device, dgf_autotune or dgf_grad2e call with the
@@ -32,7 +34,8 @@ using namespace dgf;
 namespace {
 
 constexpr int kNoAllocMaxN = 768;
-constexpr size_t kNoAllocDoubles = 3 * (size_t)kNoAllocMaxN * kNoAllocMaxN;  // 14.2 MB
+constexpr int kNoAllocMaxW = 1536;  // working functions (general contractions resolved into primitives)
+constexpr size_t kNoAllocDoubles = 3 * (size_t)kNoAllocMaxW * kNoAllocMaxW;  // 56.6 MB
 
 // The scratch of the no-allocation Fock build (see the file comment).  In
 // host code this name is only a stand-in for the device array, never a
@@ -58,25 +61,6 @@ cudaError_t scratch_address(int device, double **out) {
   return cudaSuccess;
 }
 
-__global__ void noalloc_prep_kernel(const double *__restrict__ Din, double *__restrict__ D, double *__restrict__ Ds,
-                                    int n) {
-  const int64_t n2 = (int64_t)n * n;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n2; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t p = e / n, q = e - p * n;
-    const double v = 0.5 * (Din[e] + Din[q * n + p]);
-    D[e] = v;
-    Ds[e] = 2.0 * v;
-  }
-}
-
-__global__ void noalloc_combine_kernel(const double *__restrict__ Fh, double *__restrict__ F, int n) {
-  const int64_t n2 = (int64_t)n * n;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n2; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t p = e / n, q = e - p * n;
-    F[e] = Fh[e] + Fh[q * n + p];
-  }
-}
-
 int fail(int code, int line, const std::string &msg) {
   dgf::set_error(__FILE__, line, msg);
   return code;
@@ -91,6 +75,10 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
     return fail(DGF_ERR_ARG, __LINE__,
                 "dgf_fock_device_noalloc: " + std::to_string(c->nbf) + " basis functions exceed its fixed scratch (" +
                     std::to_string(kNoAllocMaxN) + " at most); use dgf_fock_device");
+  if (c->nwf > kNoAllocMaxW)
+    return fail(DGF_ERR_ARG, __LINE__,
+                "dgf_fock_device_noalloc: " + std::to_string(c->nwf) + " working functions exceed its fixed scratch (" +
+                    std::to_string(kNoAllocMaxW) + " at most); use dgf_fock_device");
   if (c->plan.empty() || c->plan_thrs != thrs)
     return fail(DGF_ERR_ARG, __LINE__,
                 "dgf_fock_device_noalloc: no quartet plan for this threshold yet (building one needs device "
@@ -102,11 +90,11 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
   cudaError_t e = scratch_address(c->device, &scratch);
   if (e != cudaSuccess) return fail(DGF_ERR_CUDA, __LINE__, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
   cudaStream_t st = (cudaStream_t)stream;
-  const int N = c->nbf;
+  const int N = c->nwf;
   const size_t n2 = (size_t)N * N;
   double *D = scratch, *Ds = scratch + n2, *Fh = scratch + 2 * n2;
-  const int eb = 256, eg = (int)std::max<size_t>(1, std::min<size_t>((n2 + eb - 1) / eb, (size_t)c->nsm * 8));
-  noalloc_prep_kernel<<<eg, eb, 0, st>>>(dmat_device, D, Ds, N);
+  const WorkMaps maps = ctx_maps(c);
+  launch_work_prep(maps, dmat_device, D, Ds, 2, (int64_t)n2, c->nsm, st);
   e = cudaMemsetAsync(Fh, 0, n2 * sizeof(double), st);  // the accumulator starts at zero on every call
   if (e != cudaSuccess) return fail(DGF_ERR_CUDA, __LINE__, std::string("memset: ") + cudaGetErrorString(e));
   JKArgs a;
@@ -115,7 +103,7 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
   a.sph = c->d_sph;
   a.spherical = c->spherical;
   a.nbf = N;
-  a.nshell = c->nshell;
+  a.nshell = c->nwshell;
   a.slot_stride = (int64_t)n2;
   a.nslot = 1;
   a.D = D;
@@ -144,7 +132,7 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
         (int)std::max<int64_t>(1, std::min<int64_t>((cp.nquartet + per_block - 1) / per_block, (int64_t)c->nsm * 16));
     k->launch(a, grid, k->block, k->smem, st);
   }
-  noalloc_combine_kernel<<<eg, eb, 0, st>>>(Fh, fmat_device, N);
+  launch_work_combine(maps, Fh, Fh, fmat_device, 1.0, (int64_t)c->nbf * c->nbf, c->nsm, st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(DGF_ERR_CUDA, __LINE__, std::string("launch: ") + cudaGetErrorString(e));
   return DGF_OK;

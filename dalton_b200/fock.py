@@ -67,6 +67,17 @@ class FockBuilder:
         _lib.check(self._lib.dgf_info(self._h, ctypes.byref(n), ctypes.byref(a), ctypes.byref(s)), "dgf_info")
         return dict(nbf=n.value, natom=a.value, nshell=s.value)
 
+    def ao_quartets(self, thrs=1e-12) -> int:
+        """Significant contracted shell quartets of the AO basis at ``thrs``
+        (the implementation-independent size of one build)."""
+        n = _lib.dgf_int()
+        _lib.check(self._lib.dgf_count_ao_quartets(self._h, float(thrs), ctypes.byref(n)), "dgf_count_ao_quartets")
+        return int(n.value)
+
+    def copy_tuning_from(self, other: "FockBuilder"):
+        """Use the kernel choices ``other.autotune`` found."""
+        _lib.check(self._lib.dgf_copy_tuning(self._h, other._h), "dgf_copy_tuning")
+
     @staticmethod
     def _ifctyp(ifctyp, nd):
         return np.ascontiguousarray(np.broadcast_to(np.asarray(ifctyp, dtype=np.int64), (nd,)))

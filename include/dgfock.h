@@ -72,7 +72,9 @@ typedef struct {
 } dgf_basis;
 
 /* Work counters of one call (HERFCK's DINTSKP/SCRSTA statistics,
- * her2drv.F:495-541, her2gab.F:1486, in this library's units). */
+ * her2drv.F:495-541, her2gab.F:1486, in this library's units: shell quartets
+ * of the two-electron working basis, in which general contractions are
+ * resolved into primitives; dgf_count_ao_quartets gives the AO-basis count). */
 typedef struct {
   int64_t quartets_total;    /* canonical shell quartets with Q_AB*Q_CD >= thrs */
   int64_t quartets_fp64;     /* evaluated in FP64 */
@@ -133,9 +135,11 @@ int dgf_fock_device(dgf_ctx *ctx, dgf_int ndmat, const dgf_int *ifctyp, const do
  * another pool.  Same result as dgf_fock_device with ndmat = 1, IFCTYP 13,
  * ifthrs >= 20, mixed_cutoff = 0: F = J[D] - hfxfac/2 K[D] of one density
  * (symmetrised), device pointers.  Its scratch is a fixed device array of
- * 3 x 768 x 768 doubles (14.2 MB) that every GPU loading this library holds
- * until exit; contexts with more than 768 basis functions are rejected
- * (DGF_ERR_ARG).  The context's quartet plan for `thrs` must exist already
+ * 3 x 1536 x 1536 doubles (56.6 MB: density, D + D^T and half Fock matrix of
+ * the two-electron working basis, in which general contractions are resolved
+ * into primitives) that every GPU loading this library holds until exit;
+ * contexts with more than 768 basis functions, or more than 1536 working
+ * functions, are rejected (DGF_ERR_ARG).  The context's quartet plan for `thrs` must exist already
  * (an earlier dgf_fock, dgf_fock_device, dgf_autotune or dgf_grad2e call
  * with this threshold builds it), else DGF_ERR_ARG.  The first call on a
  * device looks up the array's device address; make it before any CUDA
@@ -208,8 +212,11 @@ int dgf_batch_layout(const dgf_batch *batch, dgf_int *offsets /* nmol + 1 */);
 /* J+K (IFCTYP 13, HFXFAC from opt) of every molecule of the batch, device
  * pointers to packed D and F.  use_graph = 1: the first call captures the
  * launch sequence into a CUDA graph, later calls with the same pointers,
- * options and stream replay it.  Only the FP64 Schwarz-screened form
- * (ifthrs >= 20, mixed_cutoff = 0, one shard). */
+ * options and stream replay it.  `stream` is a cudaStream_t (NULL for the
+ * legacy default stream).  Kernel choices per class come from the context
+ * with the most basis functions at dgf_batch_create time (tune it with
+ * dgf_autotune first).  Only the FP64 Schwarz-screened form (ifthrs >= 20,
+ * mixed_cutoff = 0, one shard). */
 int dgf_fock_batch(dgf_batch *batch, const double *dmat_packed_device, double *fmat_packed_device,
                    const dgf_options *opt, int use_graph, void *stream, dgf_stats *stats);
 
@@ -222,6 +229,11 @@ int dgf_fock_batch(dgf_batch *batch, const double *dmat_packed_device, double *f
 int dgf_autotune(dgf_ctx *ctx, const double *dmat_device, const dgf_options *opt, void *stream, char *report,
                  size_t report_len);
 
+/* Copy the kernel choices dgf_autotune stored in `src` to `dst` (no
+ * counterpart in Dalton), so that contexts of similar molecules share one
+ * tuning run. */
+int dgf_copy_tuning(dgf_ctx *dst, const dgf_ctx *src);
+
 /* Measurement helper (not part of the HERFCK contract): FP64 and FP32 FMA
  * throughput of device `device` in TFLOP/s from a register-resident FMA
  * loop, the denominator of the FP64-pipe roofline. */
@@ -229,6 +241,15 @@ int dgf_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
 /* Number of basis functions, atoms and segmented shells of a context. */
 int dgf_info(const dgf_ctx *ctx, dgf_int *nbf, dgf_int *natom, dgf_int *nshell);
+
+/* Workload statistic (no counterpart in Dalton): the number of contracted
+ * shell quartets of the AO basis that survive Schwarz screening at `thrs`,
+ * one shell per contracted function, canonical (A>=B, C>=D, AB>=CD).  The
+ * kernels work in a basis where general contractions are resolved into
+ * primitives, so dgf_stats.quartets_total counts that basis's quartets; this
+ * count is the implementation-independent size of the build.  Computes the
+ * AO pairs' Schwarz factors on the device on every call. */
+int dgf_count_ao_quartets(dgf_ctx *ctx, double thrs, dgf_int *count);
 
 /* Message text of a status code. */
 const char *dgf_strerror(int status);
