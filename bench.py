@@ -218,9 +218,14 @@ def run_reference(args):
 
 def best_choices(tuning):
     """Fastest candidate per class and precision from an autotune report:
-    {"la lb lc ld/precision": [variant (-1 = team kernel), ms, chunks]}."""
+    {"la lb lc ld/precision": [variant (-1 = team kernel), ms, chunks]} and the
+    mixed-form split decisions {"la lb lc ld/split": [0|1, ms FP64, ms split]}."""
     best = {}
     for r in tuning:
+        if "split" in r:  # mixed-form decision: [split?, ms FP64 only, ms FP64+FP32]
+            best[" ".join(str(x) for x in r["class"]) + "/split"] = [r["split"], round(r["ms_fp64"], 3),
+                                                                     round(r["ms_split"], 3)]
+            continue
         key = " ".join(str(x) for x in r["class"]) + f"/{r['precision']}"
         if key not in best or r["ms"] < best[key][1]:
             best[key] = [r["variant"], round(r["ms"], 3), r["chunks"]]
@@ -350,7 +355,7 @@ def main():
     H = scf64["H"]
     # Per-class kernel choice on this density (FP64 and FP32 candidates).
     t0 = time.perf_counter()
-    tuning = fb.autotune(D, thrs=THRS)
+    tuning = fb.autotune(D, thrs=THRS, mixed_cutoff=MIXED_CUTOFF)
     tune_s = time.perf_counter() - t0
     enuc = scf64["enuc"]
     # Accuracy of the mixed build at the converged density.

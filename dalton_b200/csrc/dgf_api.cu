@@ -181,7 +181,8 @@ static void free_ctx(dgf_ctx *c) {
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
   void *ptrs[] = {c->d_pairs, c->d_pp,     c->d_boys,   c->d_sph,   c->d_D,     c->d_Ds,    c->d_Fh, c->d_io,
-                  c->d_dmax,  c->d_cnt,    c->d_qoff,   c->d_wmap_i, c->d_wmap_c, c->d_wmeta, c->d_wdims, c->d_gw};
+                  c->d_dmax,  c->d_cnt,    c->d_qoff,   c->d_wmap_i, c->d_wmap_c, c->d_wmeta, c->d_wdims, c->d_gw,
+                  c->d_shinfo};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -197,20 +198,21 @@ static int cls_l1(int X) { return (X == 0) ? 0 : (X <= 2) ? 1 : (X <= 5) ? 2 : 3
 
 // Kernel for class pair (X, Y): precision 0 = FP64 (the context's choice),
 // 1 = FP32 thread kernel, 2 = FP64 team kernel (Schwarz pre-pass).
-static const ClassKernel &select_kernel(const dgf_ctx *c, int X, int Y, int precision) {
+static const ClassKernel &select_kernel(const dgf_ctx *c, int X, int Y, int precision, bool ket1) {
   if (precision == 2) return jk_kernel(X, Y, 2);
   const int p = precision ? 1 : 0;
   const int v = c->choice[X][Y][p];
-  const ClassKernel &k = jk_kernel_variant(X, Y, p, v);
+  const ClassKernel &k = jk_kernel_variant(X, Y, p, v, ket1);
   if (k.launch) return k;
-  return jk_kernel(X, Y, precision);
+  return jk_kernel(X, Y, precision, ket1);
 }
 
 static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs &args, cudaStream_t st,
                          int precision);
 
-static int launch_class(dgf_ctx *c, int X, int Y, JKArgs &args, cudaStream_t st, int precision) {
-  return launch_kernel(c, select_kernel(c, X, Y, precision), X, Y, args, st, precision);
+static int launch_class(dgf_ctx *c, int X, int Y, JKArgs &args, cudaStream_t st, int precision,
+                        bool ket1 = false) {
+  return launch_kernel(c, select_kernel(c, X, Y, precision, ket1), X, Y, args, st, precision);
 }
 
 static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs &args, cudaStream_t st,
@@ -576,6 +578,16 @@ static int upload_working_maps(dgf_ctx *c) {
   if (!cs.empty()) DGF_CUDA_CHECK(cudaMemcpy(c->d_wmap_c, cs.data(), cs.size() * 8, cudaMemcpyHostToDevice));
   DGF_CUDA_CHECK(cudaMemcpy(c->d_wmeta, meta, sizeof(meta), cudaMemcpyHostToDevice));
   DGF_CUDA_CHECK(cudaMemcpy(c->d_wdims, dims, sizeof(dims), cudaMemcpyHostToDevice));
+  std::vector<int> shinfo(c->ws_ao);
+  for (int s = 0; s < c->nwshell; ++s) shinfo.push_back(nfun(c->ws_l[s], c->spherical));
+  if (dev_alloc(&c->d_shinfo, std::max<size_t>(shinfo.size(), 1)) != cudaSuccess) {
+    cudaGetLastError();
+    DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the shell table failed");
+  }
+  if (!shinfo.empty())
+    DGF_CUDA_CHECK(cudaMemcpy(c->d_shinfo, shinfo.data(), shinfo.size() * sizeof(int), cudaMemcpyHostToDevice));
+  for (int X = 0; X < kNumPairClass; ++X)
+    for (int Y = 0; Y < kNumPairClass; ++Y) c->split_ok[X][Y] = 1;
   return DGF_OK;
 }
 
@@ -677,13 +689,16 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
   if (st) return st;
   st = compute_schwarz(c.get());
   if (st) return st;
-  // Sort each class by (primitive-count bucket, Schwarz factor descending)
+  // Sort each class by (primitive-count bucket, Schwarz bin descending, shells)
   // and record the bucket boundaries, then re-upload.
   for (int X = 0; X < kNumPairClass; ++X) {
     std::stable_sort(c->pairs.begin() + c->cls_off[X], c->pairs.begin() + c->cls_off[X + 1],
                      [](const PairRec &u, const PairRec &v) {
                        const int bu = npp_bucket(u.npp), bv = npp_bucket(v.npp);
-                       return bu != bv ? bu < bv : u.Q > v.Q;
+                       if (bu != bv) return bu < bv;
+                       const int qu = q_bin(u.Q), qv = q_bin(v.Q);
+                       if (qu != qv) return qu > qv;
+                       return u.shA != v.shA ? u.shA < v.shA : u.shB < v.shB;
                      });
     const int n = c->cls_off[X + 1] - c->cls_off[X];
     int pos = 0;
@@ -692,6 +707,18 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
       c->bkt_off[X][b] = (b == kNumBuckets) ? n : pos;
     }
   }
+  // Primitive pairs in the order of the sorted pair list.
+  {
+    std::vector<PrimPair> pp2;
+    pp2.reserve(c->pp.size());
+    for (PairRec &r : c->pairs) {
+      const int p0 = (int)pp2.size();
+      pp2.insert(pp2.end(), c->pp.begin() + r.pp0, c->pp.begin() + r.pp0 + r.npp);
+      r.pp0 = p0;
+    }
+    c->pp.swap(pp2);
+  }
+  DGF_CUDA_CHECK(cudaMemcpy(c->d_pp, c->pp.data(), c->pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice));
   DGF_CUDA_CHECK(
       cudaMemcpy(c->d_pairs, c->pairs.data(), c->pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice));
   *out = c.release();
@@ -763,7 +790,8 @@ extern "C" int dgf_count_ao_quartets(dgf_ctx *c, double thrs, dgf_int *count) {
 }
 
 // Quartet plan: for every class pair X >= Y and bra pair, the number of ket
-// pairs with Q_AB Q_CD >= thrs (a prefix of the Schwarz-sorted ket list, and
+// pairs whose Schwarz bin can reach Q_AB Q_CD >= thrs (a prefix of the
+// bin-sorted ket bucket; the kernels drop the quartets below thrs), and
 // only kets up to the bra itself when X == Y), as prefix sums.
 static int build_plan(dgf_ctx *c, double thrs) {
   if (c->plan_thrs == thrs && !c->plan.empty()) return DGF_OK;
@@ -780,6 +808,7 @@ static int build_plan(dgf_ctx *c, double thrs) {
         ClassPlan cp;
         cp.X = X;
         cp.Y = Y;
+        cp.bucket = kb;
         cp.kb0 = k0;
         cp.kb1 = k1;
         cp.off = (int64_t)all.size();
@@ -787,10 +816,10 @@ static int build_plan(dgf_ctx *c, double thrs) {
         all.push_back(0);
         for (int i = 0; i < nb; ++i) {
           const double qb = bra[i].Q;
-          int lo = k0, hi = k1;  // first ket of the bucket with qb*Q < thrs
+          int lo = k0, hi = k1;  // first ket whose whole Schwarz bin has qb*Q < thrs
           while (lo < hi) {
             int mid = (lo + hi) >> 1;
-            if (qb * ket[mid].Q >= thrs)
+            if (qb * q_bin_upper(q_bin(ket[mid].Q)) >= thrs)
               lo = mid + 1;
             else
               hi = mid;
@@ -937,14 +966,7 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   for (int k = 0; k < ndmat; ++k)
     if (outs[k].zero) DGF_CUDA_CHECK(cudaMemsetAsync(fmat_dev + (size_t)k * n2ao, 0, n2ao * 8, st));
   const int nws = c->nwshell;
-  std::vector<int> sh_nf(nws);
-  int *d_shinfo = nullptr;
-  if (need_dmax) {
-    for (int s = 0; s < nws; ++s) sh_nf[s] = nfun(c->ws_l[s], c->spherical);
-    DGF_CUDA_CHECK(dev_alloc(&d_shinfo, 2 * (size_t)nws));
-    DGF_CUDA_CHECK(cudaMemcpyAsync(d_shinfo, c->ws_ao.data(), nws * 4, cudaMemcpyHostToDevice, st));
-    DGF_CUDA_CHECK(cudaMemcpyAsync(d_shinfo + nws, sh_nf.data(), nws * 4, cudaMemcpyHostToDevice, st));
-  }
+  const int *d_shinfo = c->d_shinfo;
   for (int s0 = 0; s0 < nslot_total; s0 += chunk) {
     const int ns = std::min(chunk, nslot_total - s0);
     for (int s = 0; s < ns; ++s) {
@@ -971,6 +993,7 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     a.dmax = need_dmax ? c->d_dmax : nullptr;
     a.dens_thr = (o.ifthrs < 20) ? std::pow(10.0, -(double)o.ifthrs) : 0.0;
     a.split = o.mixed_cutoff;
+    a.schwarz_thr = o.thrs;
     a.mode = 0;
     for (const ClassPlan &cp : c->plan) {
       a.bra = c->d_pairs + c->cls_off[cp.X];
@@ -987,7 +1010,7 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
       const int lc = (cp.Y == 0) ? 0 : (cp.Y <= 2) ? 1 : (cp.Y <= 5) ? 2 : 3;
       const int ld = cp.Y - lc * (lc + 1) / 2;
       a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-      const bool split = o.mixed_cutoff > 0.0 && jk_kernel(cp.X, cp.Y, 1).launch != nullptr;
+      const bool split = o.mixed_cutoff > 0.0 && c->split_ok[cp.X][cp.Y] && jk_kernel(cp.X, cp.Y, 1).launch != nullptr;
       const int Lq = la + lb + lc + ld;
       for (int part = 0; part < (split ? 2 : 1); ++part) {
         a.mode = split ? 1 + part : 0;
@@ -995,11 +1018,8 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
         a.boys = c->d_boys + ((split && part == 1) ? boys_low_offset(Lq) : (size_t)Lq * kBoysTableDoubles);
         a.counters = c->d_cnt + 4 * (nlaunch_class % kCounterSlots);
         ++nlaunch_class;
-        int r = launch_class(c, cp.X, cp.Y, a, st, split && part == 1 ? 1 : 0);
-        if (r) {
-          if (d_shinfo) cudaFree(d_shinfo);
-          return r;
-        }
+        int r = launch_class(c, cp.X, cp.Y, a, st, split && part == 1 ? 1 : 0, cp.bucket == 0);
+        if (r) return r;
         ++launches;
       }
     }
@@ -1016,10 +1036,6 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   DGF_CUDA_CHECK(cudaEventRecord(c->ev1, st));
   st_code = finish_profile(c, st);
   if (st_code) return st_code;
-  if (d_shinfo) {
-    cudaStreamSynchronize(st);
-    cudaFree(d_shinfo);
-  }
   if (stats || c->profiling) {
     std::vector<unsigned long long> all(4 * kCounterSlots);
     DGF_CUDA_CHECK(cudaMemcpyAsync(all.data(), c->d_cnt, all.size() * 8, cudaMemcpyDeviceToHost, st));
@@ -1035,7 +1051,8 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     if (!stats) return DGF_OK;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    stats->quartets_total = total_q;
+    (void)total_q;
+    stats->quartets_total = (int64_t)(cnt[0] + cnt[2]);  // passed Schwarz: evaluated or density-skipped
     stats->quartets_fp64 = (int64_t)(cnt[0] - cnt[3]);
     stats->quartets_fp32 = (int64_t)cnt[3];
     stats->quartets_skipped = (int64_t)cnt[2];
@@ -1125,6 +1142,11 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
   r = ensure_slots(c, 1);
   if (r) return r;
   launch_work_prep(ctx_maps(c), dmat_device, c->d_D, c->d_Ds, 2, (int64_t)c->nwf * c->nwf, c->nsm, st);
+  if (o.mixed_cutoff > 0.0) {
+    const int nws = c->nwshell;
+    dmax_kernel<<<std::max(1, std::min(nws * nws / 128 + 1, c->nsm * 8)), 128, 0, st>>>(
+        c->d_D, 1, c->nwf, c->d_shinfo, c->d_shinfo + nws, nws, c->d_dmax);
+  }
   DGF_CUDA_CHECK(cudaGetLastError());
   cudaEvent_t e0, e1;
   DGF_CUDA_CHECK(cudaEventCreate(&e0));
@@ -1138,6 +1160,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
     while (jp < c->plan.size() && c->plan[jp].X == c->plan[ip].X && c->plan[jp].Y == c->plan[ip].Y) ++jp;
     const ClassPlan &cp = c->plan[ip];
     JKArgs a = base_args(c);
+    a.schwarz_thr = o.thrs;
     a.nslot = 1;
     a.D = c->d_D;
     a.Ds = c->d_Ds;
@@ -1155,8 +1178,8 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
       int bestv = c->choice[cp.X][cp.Y][p];
       a.boys = c->d_boys + (p ? boys_low_offset(la + lb + lc + ld) : (size_t)(la + lb + lc + ld) * kBoysTableDoubles);
       for (int v = -1; v < kThreadVariants; ++v) {
-        const ClassKernel &k = jk_kernel_variant(cp.X, cp.Y, p, v);
-        if (!k.launch) continue;
+        if (!jk_kernel_variant(cp.X, cp.Y, p, v).launch) continue;
+        int chunks = 1;
         float ms = 0.f;
         for (int rep2 = 0; rep2 < 2; ++rep2) {  // first pass warms caches
           DGF_CUDA_CHECK(cudaEventRecord(e0, st));
@@ -1166,6 +1189,8 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
             a.ket_off = cq.kb0;
             a.qoff = c->d_qoff + cq.off;
             a.nquartet = cq.nquartet;
+            const ClassKernel &k = jk_kernel_variant(cq.X, cq.Y, p, v, cq.bucket == 0);
+            chunks = k.chunks;
             r = launch_kernel(c, k, cq.X, cq.Y, a, st, p);
             if (r) return r;
           }
@@ -1175,7 +1200,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
         }
         char buf[160];
         snprintf(buf, sizeof(buf), "%s{\"class\":[%d,%d,%d,%d],\"precision\":%d,\"variant\":%d,\"chunks\":%d,\"ms\":%.4f}",
-                 rep.size() > 1 ? "," : "", la, lb, lc, ld, p ? 32 : 64, v, k.chunks, ms);
+                 rep.size() > 1 ? "," : "", la, lb, lc, ld, p ? 32 : 64, v, chunks, ms);
         rep += buf;
         if (ms < best) {
           best = ms;
@@ -1183,6 +1208,43 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
         }
       }
       c->choice[cp.X][cp.Y][p] = bestv;
+    }
+    // Mixed form: split the class into FP64 and FP32 launches only where
+    // that beats one FP64 pass (both walk all of the class's quartets).
+    if (o.mixed_cutoff > 0.0 && jk_kernel(cp.X, cp.Y, 1).launch) {
+      const int Lq = la + lb + lc + ld;
+      float t[2] = {0.f, 0.f};
+      for (int cfg = 0; cfg < 2; ++cfg) {  // 0: FP64 only, 1: FP64 + FP32 halves
+        for (int rep2 = 0; rep2 < 2; ++rep2) {
+          DGF_CUDA_CHECK(cudaEventRecord(e0, st));
+          for (size_t q = ip; q < jp; ++q) {
+            const ClassPlan &cq = c->plan[q];
+            a.ket = c->d_pairs + c->cls_off[cq.Y] + cq.kb0;
+            a.ket_off = cq.kb0;
+            a.qoff = c->d_qoff + cq.off;
+            a.nquartet = cq.nquartet;
+            a.dmax = c->d_dmax;
+            a.split = o.mixed_cutoff;
+            for (int part = 0; part < (cfg ? 2 : 1); ++part) {
+              const int prec = (cfg && part == 1) ? 1 : 0;
+              a.mode = cfg ? 1 + part : 0;
+              a.boys = c->d_boys + (prec ? boys_low_offset(Lq) : (size_t)Lq * kBoysTableDoubles);
+              r = launch_class(c, cq.X, cq.Y, a, st, prec, cq.bucket == 0);
+              if (r) return r;
+            }
+          }
+          DGF_CUDA_CHECK(cudaEventRecord(e1, st));
+          DGF_CUDA_CHECK(cudaEventSynchronize(e1));
+          DGF_CUDA_CHECK(cudaEventElapsedTime(&t[cfg], e0, e1));
+        }
+      }
+      a.dmax = nullptr;
+      a.mode = 0;
+      c->split_ok[cp.X][cp.Y] = t[1] < t[0] ? 1 : 0;
+      char buf[160];
+      snprintf(buf, sizeof(buf), "%s{\"class\":[%d,%d,%d,%d],\"split\":%d,\"ms_fp64\":%.4f,\"ms_split\":%.4f}",
+               rep.size() > 1 ? "," : "", la, lb, lc, ld, c->split_ok[cp.X][cp.Y], t[0], t[1]);
+      rep += buf;
     }
     ip = jp;
   }

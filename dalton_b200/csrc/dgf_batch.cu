@@ -142,16 +142,14 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
   dims.insert(dims.end(), abase.begin(), abase.end());
   std::vector<int64_t> offs(b->offsets);
   offs.insert(offs.end(), b->woffsets.begin(), b->woffsets.end());
-  std::vector<PrimPair> pp;
-  std::vector<int64_t> pp_off(nmol);
-  for (dgf_int m = 0; m < nmol; ++m) {
-    pp_off[m] = (int64_t)pp.size();
-    pp.insert(pp.end(), ctxs[m]->pp.begin(), ctxs[m]->pp.end());
-  }
-  if (pp.size() > (size_t)0x7fffffff) {
+  size_t npp_all = 0;
+  for (dgf_int m = 0; m < nmol; ++m) npp_all += ctxs[m]->pp.size();
+  if (npp_all > (size_t)0x7fffffff) {
     batch_free(b);
     BFAIL(DGF_ERR_UNSUPPORTED, "batch too large (primitive pairs exceed 2^31)");
   }
+  std::vector<PrimPair> pp;  // in the order of the merged pair list
+  pp.reserve(npp_all);
   b->mol_cls_off.assign((size_t)kNumPairClass * nmol, 0);
   for (int X = 0; X < kNumPairClass; ++X) {
     b->cls_off[X] = (int)b->pairs.size();
@@ -164,7 +162,8 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
       std::stable_sort(lst.begin(), lst.end(), [](const PairRec &u, const PairRec &v) { return u.Q > v.Q; });
       for (const PairRec &src : lst) {
         PairRec r = src;
-        r.pp0 += (int)pp_off[m];
+        r.pp0 = (int)pp.size();
+        pp.insert(pp.end(), c->pp.begin() + src.pp0, c->pp.begin() + src.pp0 + src.npp);
         r.nbfm = c->nwf;
         r.dbase = b->woffsets[m];
         b->pairs.push_back(r);

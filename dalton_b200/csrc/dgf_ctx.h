@@ -20,6 +20,7 @@ constexpr int kCounterSlots = 256;
 
 struct ClassPlan {
   int X, Y;
+  int bucket;         // primitive-count bucket of the kets (0: one primitive pair each)
   int kb0, kb1;       // ket range of this entry: one primitive-count bucket of class Y (relative to its start)
   int64_t off;        // offset of this entry's qoff array in the plan buffer
   int64_t nquartet;
@@ -56,9 +57,10 @@ struct dgf_ctx {
   int64_t *d_wmeta = nullptr;   // {0, nwf^2} {0, nbf^2} element offsets of the single-molecule form
   int *d_wdims = nullptr;       // {nwf, nbf, 0, 0}
   double *d_gw = nullptr;       // working-basis densities of the two-electron gradient (2 nwf^2)
+  int *d_shinfo = nullptr;      // per working shell: first function | function count (density bounds)
   std::vector<dgf::PairRec> pairs;  // class-major, Schwarz-descending inside a class
   int cls_off[dgf::kNumPairClass + 1] = {0};
-  // per class: bucket boundaries (relative to the class start), pairs sorted by (bucket, -Q)
+  // per class: bucket boundaries (relative to the class start), pairs sorted by (bucket, -Schwarz bin, shells)
   int bkt_off[dgf::kNumPairClass][dgf::kNumBuckets + 1] = {};
   std::vector<dgf::PrimPair> pp;
   dgf::PairRec *d_pairs = nullptr;
@@ -79,6 +81,10 @@ struct dgf_ctx {
   // kernel choice per class pair and precision (-1 = team kernel, >= 0 =
   // thread-kernel variant), set by the autotuner; 0 by default
   int choice[dgf::kNumPairClass][dgf::kNumPairClass][2] = {};
+  // mixed form: whether a class pair is split into FP64 and FP32 launches
+  // (set by the autotuner where the FP32 half pays for the second pass over
+  // the class's quartets; every class splits by default)
+  int split_ok[dgf::kNumPairClass][dgf::kNumPairClass];
   // per-class launch profiling (dgf_set_profiling)
   int profiling = 0;
   std::vector<cudaEvent_t> prof_ev;

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -20,6 +21,22 @@ constexpr int kNumBuckets = 7;  // primitive-pair-count buckets of a class list
 // lanes of a warp then loop over similar ket primitive counts.
 __host__ __device__ inline int npp_bucket(int n) {
   return n <= 1 ? 0 : n <= 2 ? 1 : n <= 4 ? 2 : n <= 8 ? 3 : n <= 16 ? 4 : n <= 32 ? 5 : 6;
+}
+
+// Schwarz bins: inside a primitive-count bucket, pairs are ordered by bin of
+// log2 Q (descending), then by shell indices, so that the kets of a warp's
+// lanes are neighbours in the density and Fock matrices.  A bra's significant
+// kets are then a prefix of whole bins, and the kernels drop the few quartets
+// of the last bin below the threshold.
+constexpr int kQBinsPerOctave = 2;
+inline int q_bin(double q) {
+  if (!(q > 0.0)) return -(1 << 20);
+  int e = 0;
+  const double m = std::frexp(q, &e);  // q = m 2^e, m in [0.5, 1)
+  return (int)std::floor(((double)e + std::log2(m)) * kQBinsPerOctave);
+}
+inline double q_bin_upper(int bin) {  // every Q of the bin is below this
+  return bin <= -(1 << 20) ? 0.0 : std::exp2((double)(bin + 1) / kQBinsPerOctave);
 }
 
 // Boys-function table: F_M(T) on [0, kBoysTmax) in kBoysNint intervals of
@@ -47,23 +64,29 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 // Primitive pair of a shell pair (A first, the higher angular momentum).
 // K = c_a c_b exp(-mu |AB|^2) sqrt(2 pi^(5/2)) / p, Dalton's FAC12 with R2PI52
-// (DALTON/abacus/her2odc.F:229-231, DALTON/include/pi.h:9-14).
-struct PrimPair {
+// (DALTON/abacus/her2odc.F:229-231, DALTON/include/pi.h:9-14).  96 bytes,
+// 16-byte aligned so that a lane reads one with 128-bit loads; the primitive
+// pairs of a context are stored in the order of the class-sorted pair list,
+// so the kets of consecutive lanes are adjacent in memory.
+struct __align__(16) PrimPair {
   double p, Px, Py, Pz, PAx, PAy, PAz, PBx, PBy, PBz, K, ea;  // ea: exponent of A (B's is p - ea)
 };
 
-// Shell pair record in a class list (sorted by Schwarz factor, descending).
-struct PairRec {
-  int shA, shB;    // segmented shell indices (A has l >= l of B)
-  int aoA, aoB;    // first AO of each shell (within its molecule)
+// Shell pair record in a class list (sorted by Schwarz factor, descending),
+// 64 bytes in four 16-byte groups, the fields every quartet reads first.
+struct __align__(16) PairRec {
+  int aoA, aoB;    // first function of each shell (within its molecule's working basis)
   int pp0, npp;    // primitive-pair range
   int same;        // A == B
-  int atA;         // atom of A (atom of B in atB)
-  int atB;
+  int shA, shB;    // working-basis shell indices (A has l >= l of B)
   int nbfm;        // basis size of the pair's molecule (row stride of its D/F blocks)
   double Q;        // Schwarz factor sqrt(max |(ab|ab)|)
   int64_t dbase;   // offset of the molecule's N x N block in packed D/F storage (0 for one molecule)
+  int atA, atB;    // atoms of A and B
+  int pad0, pad1;
 };
+
+static_assert(sizeof(PrimPair) == 96 && sizeof(PairRec) == 64, "pair records are read 16 bytes at a time");
 
 // Arguments of one quartet-class launch.
 struct JKArgs {
@@ -93,6 +116,7 @@ struct JKArgs {
   int nshell;
   double dens_thr;          // skip if bound < dens_thr (0: no density screening)
   double split;             // precision split bound
+  double schwarz_thr;       // skip quartets with Q_AB Q_CD below this (0: the plan is exact)
   int mode;                 // 0: all, 1: bound >= split only, 2: bound < split only
   double *diag_out;         // Schwarz mode: sqrt(max |(ab|ab)|) per bra pair, no digestion
   unsigned long long *counters;  // [0] quartets done, [1] primitive quartets, [2] skipped
@@ -100,6 +124,7 @@ struct JKArgs {
   const double *G1, *G2;
   double *grad;
   double hfx;
+  int natom;
 };
 
 // Offset of the l-block of the Cartesian->spherical table: rows m=-l..l,
@@ -124,9 +149,11 @@ constexpr int kThreadVariants = 2;
 
 // Per-class launch table (filled by dgf_jk.cu): index [X][Y] of pair classes.
 // precision: 0 = default FP64 kernel, 1 = FP32 thread kernel, 2 = team kernel.
-const ClassKernel &jk_kernel(int X, int Y, int precision);
+// ket1: the launch's kets have one primitive pair each (thread kernels then
+// use their single-ket-primitive form).
+const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1 = false);
 // variant -1 = team kernel, >= 0 = thread-kernel variant (precision 0/1).
-const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant);
+const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1 = false);
 cudaError_t jk_prepare_all();
 
 void boys_table_host(std::vector<double> &out);       // [kBoysMaxM+1][kBoysTableDoubles]

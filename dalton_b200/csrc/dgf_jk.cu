@@ -15,18 +15,22 @@ const ClassKernel kNone{nullptr, 0, 0, 0};
 
 // variant: -1 = team kernel, 0.. = thread-kernel variant; precision 0 = FP64,
 // 1 = FP32.  Returns a kernel with launch == nullptr when absent.
-const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant) {
+const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1) {
   const JKEntry &e = g_jk_table[X][Y];
   if (variant < 0) return precision == 0 ? e.team : kNone;
   if (variant >= kThreadVariants) return kNone;
-  return e.thr[precision ? 1 : 0][variant];
+  const int p = precision ? 1 : 0;
+  if (ket1 && e.thr1[p][variant].launch) return e.thr1[p][variant];
+  return e.thr[p][variant];
 }
 
 // Default choice: first thread variant when the class has one, else team.
-const ClassKernel &jk_kernel(int X, int Y, int precision) {
+const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1) {
   const JKEntry &e = g_jk_table[X][Y];
-  if (precision == 1) return e.thr[1][0];
   if (precision == 2) return e.team;
+  const int p = precision == 1 ? 1 : 0;
+  if (ket1 && e.thr1[p][0].launch) return e.thr1[p][0];
+  if (precision == 1) return e.thr[1][0];
   return e.thr[0][0].launch ? e.thr[0][0] : e.team;
 }
 

@@ -11,7 +11,8 @@ namespace dgf {
 
 struct JKEntry {
   ClassKernel team;
-  ClassKernel thr[2][kThreadVariants];  // [precision 0 = FP64, 1 = FP32][variant]
+  ClassKernel thr[2][kThreadVariants];   // [precision 0 = FP64, 1 = FP32][variant]
+  ClassKernel thr1[2][kThreadVariants];  // same, for kets of one primitive pair each
   cudaError_t (*prepare)();
 };
 
@@ -40,9 +41,9 @@ void launch_team(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t
   jk_team_kernel<LA, LB, LC, LD><<<grid, block, smem, s>>>(a);
 }
 
-template <int LA, int LB, int LC, int LD, typename T, int CA>
+template <int LA, int LB, int LC, int LD, typename T, int CA, int K1>
 void launch_thread(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
-  jk_thread_kernel<LA, LB, LC, LD, T, CA><<<dim3(grid, CA), block, smem, s>>>(a);
+  jk_thread_kernel<LA, LB, LC, LD, T, CA, K1><<<dim3(grid, CA), block, smem, s>>>(a);
 }
 
 template <int LA, int LB, int LC, int LD>
@@ -51,9 +52,9 @@ cudaError_t prepare_team() {
                               (int)TeamShape<LA, LB, LC, LD>::smem());
 }
 
-template <int LA, int LB, int LC, int LD, typename T, int CA>
+template <int LA, int LB, int LC, int LD, typename T, int CA, int K1 = 0>
 ClassKernel thread_entry() {
-  return ClassKernel{&launch_thread<LA, LB, LC, LD, T, CA>, kThreadBlock, 0, CA};
+  return ClassKernel{&launch_thread<LA, LB, LC, LD, T, CA, K1>, kThreadBlock, 0, CA};
 }
 
 template <int X, int Y>
@@ -66,7 +67,7 @@ void fill_one() {
   e.team = ClassKernel{&launch_team<LA, LB, LC, LD>, block, S::smem(), 1};
   e.prepare = &prepare_team<LA, LB, LC, LD>;
   for (int p = 0; p < 2; ++p)
-    for (int v = 0; v < kThreadVariants; ++v) e.thr[p][v] = ClassKernel{nullptr, 0, 0, 0};
+    for (int v = 0; v < kThreadVariants; ++v) e.thr[p][v] = e.thr1[p][v] = ClassKernel{nullptr, 0, 0, 0};
   if constexpr (thread_eligible(LA, LB, LC, LD)) {
     constexpr int c64 = chunks_for(LA, LB, LC, LD, 27), c64b = cmin(ncart(LA), 2 * c64);
     constexpr int c32 = chunks_for(LA, LB, LC, LD, 54), c32b = cmin(ncart(LA), 2 * c32);
@@ -74,6 +75,10 @@ void fill_one() {
     e.thr[1][0] = thread_entry<LA, LB, LC, LD, float, c32>();
     if constexpr (c64b != c64) e.thr[0][1] = thread_entry<LA, LB, LC, LD, double, c64b>();
     if constexpr (c32b != c32) e.thr[1][1] = thread_entry<LA, LB, LC, LD, float, c32b>();
+    e.thr1[0][0] = thread_entry<LA, LB, LC, LD, double, c64, 1>();
+    e.thr1[1][0] = thread_entry<LA, LB, LC, LD, float, c32, 1>();
+    if constexpr (c64b != c64) e.thr1[0][1] = thread_entry<LA, LB, LC, LD, double, c64b, 1>();
+    if constexpr (c32b != c32) e.thr1[1][1] = thread_entry<LA, LB, LC, LD, float, c32b, 1>();
   }
 }
 

@@ -26,8 +26,10 @@ __device__ __forceinline__ double quartet_bound(const JKArgs &a, const PairRec &
   return b.Q * k.Q * (double)fmaxf(4.0f * dj, dk);
 }
 
-// Returns 0 = evaluate, 1 = outside this launch's precision range, 2 = screened out.
+// Returns 0 = evaluate, 1 = outside this launch's precision range, 2 = screened
+// out by the density bound, 3 = below the Schwarz threshold (the plan's last bin).
 __device__ __forceinline__ int quartet_select(const JKArgs &a, const PairRec &b, const PairRec &k) {
+  if (b.Q * k.Q < a.schwarz_thr) return 3;
   if (!a.dmax) return 0;
   double bound = quartet_bound(a, b, k);
   if (bound < a.dens_thr) return 2;

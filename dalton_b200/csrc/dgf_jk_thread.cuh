@@ -27,13 +27,11 @@ namespace dgf {
 // J_cd, K_ac, K_ad, K_bc, K_bd as FP64 atomics into the half Fock matrices.
 template <int FA, int FB, int FC, int FD>
 __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool work, bool uniform, int ib, int ic,
-                                          int ib0, const PairRec &kt, int a_off) {
+                                          int ib0, const PairRec &br, const PairRec &kt, int a_off) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   double w = 0.0;
-  PairRec br;
   if (work) {
-    br = a.bra[ib];
     w = 1.0;
     if (br.same) w *= 0.5;
     if (kt.same) w *= 0.5;
@@ -42,7 +40,7 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
   // The warp's bra pair (valid on every lane) for the warp-reduced J_ab block;
   // a quartet's bra and ket belong to one molecule, so its N x N block is
   // the bra's.
-  const PairRec brw = a.bra[ib0];
+  const PairRec brw = load_pair(a.bra + ib0);
   const int N = work ? br.nbfm : brw.nbfm;
   const int64_t db = work ? br.dbase : brw.dbase;
   for (int k = 0; k < a.nslot; ++k) {
@@ -142,7 +140,7 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
 constexpr int kThreadBlock = 128;
 constexpr int kThreadWarps = kThreadBlock / 32;
 
-template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH>
+template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, const double *sph, Tc *ebra,
                                                unsigned long long &cnt_q, unsigned long long &cnt_p,
                                                unsigned long long &cnt_s) {
@@ -159,15 +157,32 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
   constexpr int NOUT = cmax(NACC, cmax(FAc, NAc) * cmax(NB, FBc) * cmax(NC, FCc) * cmax(ND, FDc));
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = a.q_begin + (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.nquartet;
-       base += stride) {
+  // Each warp takes one contiguous range of the queue (a multiple of 32
+  // quartets), so its bra index only moves forward: one binary search per
+  // warp, then a short walk along qoff per 32 quartets.
+  const int64_t nwarp = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t span = (((a.nquartet - a.q_begin) + nwarp - 1) / nwarp + 31) & ~(int64_t)31;
+  const int64_t wbegin = a.q_begin + wid * span, wend = min(wbegin + span, a.nquartet);
+  int ibw = 0;
+  if (wbegin < wend && lane == 0) ibw = find_bra(a.qoff, a.nbra, wbegin);
+  ibw = __shfl_sync(full, ibw, 0);
+  for (int64_t base = wbegin; base < wend; base += 32) {
     const int64_t q = base + lane;
-    const bool active = q < a.nquartet;
-    int ib0 = 0;
-    if (lane == 0) ib0 = find_bra(a.qoff, a.nbra, base);
+    const bool active = q < wend;
+    int ib0 = ibw;
+    if (lane == 0) {  // the warp's first bra: a short walk, else a search
+      int steps = 0;
+      while (base >= a.qoff[ib0 + 1] && steps < 32) {
+        ++ib0;
+        ++steps;
+      }
+      if (base >= a.qoff[ib0 + 1]) ib0 = find_bra(a.qoff, a.nbra, base);
+    }
     ib0 = __shfl_sync(full, ib0, 0);
+    ibw = ib0;
     int ib = ib0, ic = 0, sel = 1;
+    PairRec br, kt;
     if (active) {
       int steps = 0;
       while (q >= a.qoff[ib + 1] && steps < 32) {
@@ -176,15 +191,17 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
       }
       if (q >= a.qoff[ib + 1]) ib = find_bra(a.qoff, a.nbra, q);
       ic = (int)(q - a.qoff[ib]) + (a.kbase ? a.kbase[ib] : 0);
-      sel = quartet_select(a, a.bra[ib], a.ket[ic]);
-      if (sel == 2 && CH == 0) ++cnt_s;
+      br = load_pair(a.bra + ib);
+      kt = load_pair(a.ket + ic);
+      sel = quartet_select(a, br, kt);
+      if (sel == 2 && CH == 0 && a.mode != 2) ++cnt_s;  // a split class counts its skips in the FP64 launch
     }
     const bool work = active && sel == 0;
     Tc acc[NACC];
 #pragma unroll
     for (int k = 0; k < NACC; ++k) acc[k] = Tc(0);
-    PairRec kt;
-    if (work) kt = a.ket[ic];
+    PrimPair P2one;  // K1: the ket's only primitive pair, fetched before the bra work
+    if (K1 && work) P2one = load_prim<(LC + LD > 0)>(a.pp + kt.pp0);
     // Bra groups: lanes sharing a bra pair run its primitive loop together.
     unsigned pending = __ballot_sync(full, work);
     while (pending) {
@@ -192,9 +209,9 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
       const int ibl = __shfl_sync(full, ib, leader);
       const bool mine = work && ib == ibl && ((pending >> lane) & 1u);
       pending &= ~__ballot_sync(full, mine);
-      const PairRec brl = a.bra[ibl];
+      const PairRec brl = load_pair(a.bra + ibl);
       for (int i = 0; i < brl.npp; ++i) {
-        const PrimPair P1 = a.pp[brl.pp0 + i];
+        const PrimPair P1 = load_prim<true>(a.pp + brl.pp0 + i);
         __syncwarp();
         if (lane < 3) {
           const Tc h1 = Tc(0.5 / P1.p);
@@ -274,21 +291,23 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
                 }
             }
         };
-        if constexpr (L <= 2) {
+        if constexpr (K1 != 0) {
+          ket_prim(P2one);  // kets of this launch have one primitive pair each
+        } else if constexpr (L <= 2) {
           // two independent primitive quartets per iteration for latency hiding
           int j = 0;
           for (; j + 1 < kt.npp; j += 2) {
-            const PrimPair P2a = a.pp[kt.pp0 + j];
-            const PrimPair P2b = a.pp[kt.pp0 + j + 1];
+            const PrimPair P2a = load_prim<(LC + LD > 0)>(a.pp + kt.pp0 + j);
+            const PrimPair P2b = load_prim<(LC + LD > 0)>(a.pp + kt.pp0 + j + 1);
             ket_prim(P2a);
             ket_prim(P2b);
           }
-          if (j < kt.npp) ket_prim(a.pp[kt.pp0 + j]);
+          if (j < kt.npp) ket_prim(load_prim<(LC + LD > 0)>(a.pp + kt.pp0 + j));
         } else {
-          PrimPair nxt = a.pp[kt.pp0];
+          PrimPair nxt = load_prim<(LC + LD > 0)>(a.pp + kt.pp0);
           for (int j = 0; j < kt.npp; ++j) {
             const PrimPair P2 = nxt;  // the next ket primitive pair is fetched during this one's arithmetic
-            if (j + 1 < kt.npp) nxt = a.pp[kt.pp0 + j + 1];
+            if (j + 1 < kt.npp) nxt = load_prim<(LC + LD > 0)>(a.pp + kt.pp0 + j + 1);
             ket_prim(P2);
           }
         }
@@ -296,7 +315,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
     }
     if (work) {
       cnt_q += (CH == 0);
-      if (CH == 0) cnt_p += (unsigned long long)a.bra[ib].npp * kt.npp;
+      if (CH == 0) cnt_p += (unsigned long long)br.npp * kt.npp;
     }
     // Chunk block -> the shells' functions: spherical A (partial sums over
     // this chunk's Cartesian components), then B, C, D.
@@ -376,26 +395,41 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
     const bool uniform = __all_sync(full, !work || ib == ib0) && __any_sync(full, work);
     if (!__any_sync(full, work)) continue;
     if (sphr)
-      jk_digest<FAc, FBc, FCc, FDc>(a, g, work, uniform, ib, ic, ib0, kt, 0);
+      jk_digest<FAc, FBc, FCc, FDc>(a, g, work, uniform, ib, ic, ib0, br, kt, 0);
     else
-      jk_digest<NAc, NB, NC, ND>(a, g, work, uniform, ib, ic, ib0, kt, A0);
+      jk_digest<NAc, NB, NC, ND>(a, g, work, uniform, ib, ic, ib0, br, kt, A0);
   }
 }
 
-template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH>
+template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, const double *tab, const double *sph,
                                                    Tc *ebra, unsigned long long &q, unsigned long long &p,
                                                    unsigned long long &s) {
   if constexpr (CH < CA) {
     if (chunk == CH)
-      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH>(a, tab, sph, ebra, q, p, s);
+      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, sph, ebra, q, p, s);
     else
-      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1>(chunk, a, tab, sph, ebra, q, p, s);
+      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, sph, ebra, q, p, s);
   }
 }
 
-template <int LA, int LB, int LC, int LD, typename Tc, int CA>
-__global__ void __launch_bounds__(kThreadBlock) jk_thread_kernel(const JKArgs a) {
+// Resident blocks per SM the register allocation must allow: the low-L
+// classes are latency bound (few FLOPs per quartet, long chains of dependent
+// loads), so they trade registers for warps.
+#ifndef DGF_THREAD_MINB_L2
+#define DGF_THREAD_MINB_L2 4
+#endif
+#ifndef DGF_THREAD_MINB_L3
+#define DGF_THREAD_MINB_L3 1
+#endif
+constexpr int thread_min_blocks(int L) { return L <= 2 ? DGF_THREAD_MINB_L2 : L == 3 ? DGF_THREAD_MINB_L3 : 1; }
+
+// K1 = 1: every ket pair of the launch has exactly one primitive pair (the
+// first primitive-count bucket; all pairs of a basis whose general
+// contractions are resolved into primitives), so the ket loop collapses.
+template <int LA, int LB, int LC, int LD, typename Tc, int CA, int K1>
+__global__ void __launch_bounds__(kThreadBlock, thread_min_blocks(LA + LB + LC + LD))
+    jk_thread_kernel(const JKArgs a) {
   constexpr int EA = (LA + 1) * (LB + 1) * (LA + LB + 1);
   __shared__ double tab[kBoysTableDoubles];
   __shared__ double sph[kSphTableDoubles];
@@ -404,7 +438,7 @@ __global__ void __launch_bounds__(kThreadBlock) jk_thread_kernel(const JKArgs a)
   for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
   __syncthreads();
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
-  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0>(blockIdx.y, a, tab, sph, ebra_all[threadIdx.x >> 5], cnt_q, cnt_p,
+  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, sph, ebra_all[threadIdx.x >> 5], cnt_q, cnt_p,
                                                 cnt_s);
   if (a.counters) {
     const int lane = threadIdx.x & 31;

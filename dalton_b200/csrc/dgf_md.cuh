@@ -118,6 +118,36 @@ __device__ __forceinline__ void herm_e(T h, T pa, T pb, T *E) {
 }
 
 // Maps a flattened quartet index to (bra, ket) through the prefix array.
+// Pair records through the read-only data path, 16 bytes at a time (the
+// records are 16-byte aligned); load_prim<false> skips P-A and P-B, which
+// (ss) pairs do not use.
+__device__ __forceinline__ PairRec load_pair(const PairRec *p) {
+  PairRec r;
+  const int4 *s = reinterpret_cast<const int4 *>(p);
+  int4 *d = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(PairRec) / 16); ++k) d[k] = __ldg(s + k);
+  return r;
+}
+
+template <bool PAB>
+__device__ __forceinline__ PrimPair load_prim(const PrimPair *p) {
+  PrimPair r;
+  const double2 *s = reinterpret_cast<const double2 *>(p);
+  double2 *d = reinterpret_cast<double2 *>(&r);
+  d[0] = __ldg(s + 0);  // p, Px
+  d[1] = __ldg(s + 1);  // Py, Pz
+  if (PAB) {
+    d[2] = __ldg(s + 2);  // PAx, PAy
+    d[3] = __ldg(s + 3);  // PAz, PBx
+    d[4] = __ldg(s + 4);  // PBy, PBz
+  } else {
+    d[2] = d[3] = d[4] = make_double2(0.0, 0.0);
+  }
+  d[5] = __ldg(s + 5);  // K, ea
+  return r;
+}
+
 __device__ __forceinline__ int find_bra(const int64_t *__restrict__ qoff, int nbra, int64_t q) {
   int lo = 0, hi = nbra;
   while (hi - lo > 1) {

@@ -111,6 +111,7 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
   a.Fh = Fh;
   a.jscale[0] = 1.0;
   a.kscale[0] = 0.5 * hfxfac;
+  a.schwarz_thr = thrs;
   for (const ClassPlan &cp : c->plan) {
     a.bra = c->d_pairs + c->cls_off[cp.X];
     a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
@@ -125,8 +126,8 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
     const int lc = (cp.Y == 0) ? 0 : (cp.Y <= 2) ? 1 : (cp.Y <= 5) ? 2 : 3;
     const int ld = cp.Y - lc * (lc + 1) / 2;
     a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-    const ClassKernel *k = &jk_kernel_variant(cp.X, cp.Y, 0, c->choice[cp.X][cp.Y][0]);
-    if (!k->launch) k = &jk_kernel(cp.X, cp.Y, 0);
+    const ClassKernel *k = &jk_kernel_variant(cp.X, cp.Y, 0, c->choice[cp.X][cp.Y][0], cp.bucket == 0);
+    if (!k->launch) k = &jk_kernel(cp.X, cp.Y, 0, cp.bucket == 0);
     const int64_t per_block = (k->smem == 0) ? k->block : 1;
     const int grid =
         (int)std::max<int64_t>(1, std::min<int64_t>((cp.nquartet + per_block - 1) / per_block, (int64_t)c->nsm * 16));

@@ -128,15 +128,17 @@ class FockBuilder:
             self.last_stats = st.as_dict()
         return fmat
 
-    def autotune(self, dmat, thrs=1e-12, hfxfac=1.0):
+    def autotune(self, dmat, thrs=1e-12, hfxfac=1.0, mixed_cutoff=0.0):
         """Time every candidate kernel per quartet class on this density (a
-        CUDA float64 tensor) and keep the fastest; returns the timing list."""
+        CUDA float64 tensor) and keep the fastest; with ``mixed_cutoff`` > 0
+        also decide per class whether the mixed form splits it into FP64 and
+        FP32 launches.  Returns the timing list."""
         import json
 
         import torch
 
         d = dmat.contiguous()
-        opt = _lib.default_options(thrs=float(thrs), hfxfac=float(hfxfac))
+        opt = _lib.default_options(thrs=float(thrs), hfxfac=float(hfxfac), mixed_cutoff=float(mixed_cutoff))
         buf = ctypes.create_string_buffer(1 << 16)
         stream = torch.cuda.current_stream(d.device).cuda_stream
         _lib.check(self._lib.dgf_autotune(self._h, ctypes.c_void_p(d.data_ptr()), ctypes.byref(opt),
