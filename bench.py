@@ -216,6 +216,20 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def ncu_traffic(kernel, workload):
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of
+    `kernel` on `workload`, as recorded from an ncu capture of the same
+    command in profiles/traffic.txt (lines: kernel workload bytes), or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 3 and not line.startswith("#") and f[0] == kernel and f[1] == workload:
+            return float(f[2])
+    return None
+
+
 def best_choices(tuning):
     """Fastest candidate per class and precision from an autotune report:
     {"la lb lc ld/precision": [variant (-1 = team kernel), ms, chunks]} and the
@@ -459,7 +473,10 @@ def main():
                           f"{top['lc']},{top['ld']},{'double' if top['precision'] == 64 else 'float'}>",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": "measured FMA-loop peak on this GPU (MEASURED_PEAKS.json has no FP64 figure)",
-                "traffic": None, "share_of_build": top["ms"] / tot_ms if tot_ms else None,
+                "traffic": ncu_traffic(f"jk_{'thread' if top['kernel'] == 0 else 'team'}_kernel<{top['la']},{top['lb']},"
+                                       f"{top['lc']},{top['ld']},{'double' if top['precision'] == 64 else 'float'}>",
+                                       args.workload),
+                "share_of_build": top["ms"] / tot_ms if tot_ms else None,
                 "flops_model": "dalton_b200/perfmodel.py (per primitive and per contracted quartet)"}
     all_flops = sum(class_flops(r["la"], r["lb"], r["lc"], r["ld"], r["prim_quartets"], r["evaluated"]) for r in prof)
     build_tflops = all_flops / (tot_ms * 1e-3) / 1e12 if tot_ms else None

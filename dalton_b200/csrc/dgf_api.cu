@@ -1010,7 +1010,8 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
       const int lc = (cp.Y == 0) ? 0 : (cp.Y <= 2) ? 1 : (cp.Y <= 5) ? 2 : 3;
       const int ld = cp.Y - lc * (lc + 1) / 2;
       a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-      const bool split = o.mixed_cutoff > 0.0 && c->split_ok[cp.X][cp.Y] && jk_kernel(cp.X, cp.Y, 1).launch != nullptr;
+      const bool split = o.mixed_cutoff > 0.0 && c->split_ok[cp.X][cp.Y] &&
+                         jk_kernel(cp.X, cp.Y, 1, cp.bucket == 0).launch != nullptr;
       const int Lq = la + lb + lc + ld;
       for (int part = 0; part < (split ? 2 : 1); ++part) {
         a.mode = split ? 1 + part : 0;
@@ -1178,7 +1179,8 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
       int bestv = c->choice[cp.X][cp.Y][p];
       a.boys = c->d_boys + (p ? boys_low_offset(la + lb + lc + ld) : (size_t)(la + lb + lc + ld) * kBoysTableDoubles);
       for (int v = -1; v < kThreadVariants; ++v) {
-        if (!jk_kernel_variant(cp.X, cp.Y, p, v).launch) continue;
+        if (!jk_kernel_variant(cp.X, cp.Y, p, v).launch && !jk_kernel_variant(cp.X, cp.Y, p, v, true).launch)
+          continue;
         int chunks = 1;
         float ms = 0.f;
         for (int rep2 = 0; rep2 < 2; ++rep2) {  // first pass warms caches
@@ -1189,9 +1191,11 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
             a.ket_off = cq.kb0;
             a.qoff = c->d_qoff + cq.off;
             a.nquartet = cq.nquartet;
-            const ClassKernel &k = jk_kernel_variant(cq.X, cq.Y, p, v, cq.bucket == 0);
-            chunks = k.chunks;
-            r = launch_kernel(c, k, cq.X, cq.Y, a, st, p);
+            // entries this candidate has no kernel for run the FP64 default (same for every candidate)
+            const ClassKernel &kv = jk_kernel_variant(cq.X, cq.Y, p, v, cq.bucket == 0);
+            const ClassKernel &k = kv.launch ? kv : jk_kernel(cq.X, cq.Y, 0, cq.bucket == 0);
+            if (kv.launch) chunks = k.chunks;
+            r = launch_kernel(c, k, cq.X, cq.Y, a, st, kv.launch ? p : 0);
             if (r) return r;
           }
           DGF_CUDA_CHECK(cudaEventRecord(e1, st));
@@ -1211,7 +1215,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
     }
     // Mixed form: split the class into FP64 and FP32 launches only where
     // that beats one FP64 pass (both walk all of the class's quartets).
-    if (o.mixed_cutoff > 0.0 && jk_kernel(cp.X, cp.Y, 1).launch) {
+    if (o.mixed_cutoff > 0.0 && (jk_kernel(cp.X, cp.Y, 1).launch || jk_kernel(cp.X, cp.Y, 1, true).launch)) {
       const int Lq = la + lb + lc + ld;
       float t[2] = {0.f, 0.f};
       for (int cfg = 0; cfg < 2; ++cfg) {  // 0: FP64 only, 1: FP64 + FP32 halves
@@ -1225,9 +1229,11 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
             a.nquartet = cq.nquartet;
             a.dmax = c->d_dmax;
             a.split = o.mixed_cutoff;
-            for (int part = 0; part < (cfg ? 2 : 1); ++part) {
+            // as in the build: entries without an FP32 kernel are not split
+            const bool cansplit = jk_kernel(cq.X, cq.Y, 1, cq.bucket == 0).launch != nullptr;
+            for (int part = 0; part < (cfg && cansplit ? 2 : 1); ++part) {
               const int prec = (cfg && part == 1) ? 1 : 0;
-              a.mode = cfg ? 1 + part : 0;
+              a.mode = (cfg && cansplit) ? 1 + part : 0;
               a.boys = c->d_boys + (prec ? boys_low_offset(Lq) : (size_t)Lq * kBoysTableDoubles);
               r = launch_class(c, cq.X, cq.Y, a, st, prec, cq.bucket == 0);
               if (r) return r;

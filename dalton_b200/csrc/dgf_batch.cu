@@ -4,7 +4,9 @@
 //
 // Every molecule keeps its own canonical quartet list (no cross-molecule
 // quartets): the merged pair list of a class is the concatenation of the
-// molecules' Schwarz-sorted lists, each pair record carries its molecule's
+// molecules' lists in their contexts' order (primitive-count bucket, Schwarz
+// bin, shells), the plan has one entry per (class pair, ket bucket) over
+// every molecule's bras, each pair record carries its molecule's
 // offset and size in the packed working-basis D/F storage, and the plan
 // stores, per bra pair, the first ket of its molecule in the merged ket
 // list.  The packed AO-basis matrices of the caller are mapped to and from
@@ -21,6 +23,7 @@ using namespace dgf;
 
 struct BatchPlan {
   int X, Y;
+  int bucket;        // primitive-count bucket of the kets (0: one primitive pair each)
   int64_t off;       // into the qoff buffer (nbra+1 entries)
   int64_t koff;      // into the kbase buffer (nbra entries)
   int64_t nquartet;
@@ -35,6 +38,7 @@ struct dgf_batch {
   std::vector<PairRec> pairs;
   int cls_off[kNumPairClass + 1] = {0};
   std::vector<int> mol_cls_off;  // [X * nmol + m]: start of molecule m's class-X pairs in the merged list
+  std::vector<int> mol_bkt;      // [(X * nmol + m) * (kNumBuckets + 1) + k]: bucket starts inside that list
   PairRec *d_pairs = nullptr;
   PrimPair *d_pp = nullptr;
   double *d_boys = nullptr, *d_sph = nullptr;
@@ -151,15 +155,17 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
   std::vector<PrimPair> pp;  // in the order of the merged pair list
   pp.reserve(npp_all);
   b->mol_cls_off.assign((size_t)kNumPairClass * nmol, 0);
+  b->mol_bkt.assign((size_t)kNumPairClass * nmol * (kNumBuckets + 1), 0);
   for (int X = 0; X < kNumPairClass; ++X) {
     b->cls_off[X] = (int)b->pairs.size();
     for (dgf_int m = 0; m < nmol; ++m) {
       const dgf_ctx *c = ctxs[m];
       b->mol_cls_off[(size_t)X * nmol + m] = (int)b->pairs.size();
-      // The batch plan takes each bra's partners as a Schwarz prefix of its
-      // molecule's class list, so the list is ordered by Q alone here.
+      // The molecule's class list in its context's order: primitive-count
+      // bucket, Schwarz bin, shells (a bra's partners in one bucket are a
+      // prefix of whole bins).
+      for (int k = 0; k <= kNumBuckets; ++k) b->mol_bkt[((size_t)X * nmol + m) * (kNumBuckets + 1) + k] = c->bkt_off[X][k];
       std::vector<PairRec> lst(c->pairs.begin() + c->cls_off[X], c->pairs.begin() + c->cls_off[X + 1]);
-      std::stable_sort(lst.begin(), lst.end(), [](const PairRec &u, const PairRec &v) { return u.Q > v.Q; });
       for (const PairRec &src : lst) {
         PairRec r = src;
         r.pp0 = (int)pp.size();
@@ -246,40 +252,50 @@ static int batch_plan(dgf_batch *b, double thrs) {
     return (m + 1 < nm) ? b->mol_cls_off[(size_t)X * nm + m + 1] : b->cls_off[X + 1];
   };
   for (int X = 0; X < kNumPairClass; ++X)
-    for (int Y = 0; Y <= X; ++Y) {
-      const int nb = b->cls_off[X + 1] - b->cls_off[X];
-      const int nk = b->cls_off[Y + 1] - b->cls_off[Y];
-      if (!nb || !nk) continue;
-      BatchPlan bp;
-      bp.X = X;
-      bp.Y = Y;
-      bp.off = (int64_t)qoff.size();
-      bp.koff = (int64_t)kbase.size();
-      int64_t acc = 0;
-      qoff.push_back(0);
-      for (int m = 0; m < nm; ++m) {
-        const int b0 = b->mol_cls_off[(size_t)X * nm + m], b1 = mol_end(X, m);
-        const int k0 = b->mol_cls_off[(size_t)Y * nm + m], k1 = mol_end(Y, m);
-        for (int i = b0; i < b1; ++i) {
-          const double qb = b->pairs[i].Q;
-          int lo = k0, hi = k1;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (qb * b->pairs[mid].Q >= thrs)
-              lo = mid + 1;
-            else
-              hi = mid;
+    for (int Y = 0; Y <= X; ++Y)
+      for (int kb = 0; kb < kNumBuckets; ++kb) {
+        const int nb = b->cls_off[X + 1] - b->cls_off[X];
+        const int nk = b->cls_off[Y + 1] - b->cls_off[Y];
+        if (!nb || !nk) continue;
+        BatchPlan bp;
+        bp.X = X;
+        bp.Y = Y;
+        bp.bucket = kb;
+        bp.off = (int64_t)qoff.size();
+        bp.koff = (int64_t)kbase.size();
+        int64_t acc = 0;
+        qoff.push_back(0);
+        for (int m = 0; m < nm; ++m) {
+          const int b0 = b->mol_cls_off[(size_t)X * nm + m], b1 = mol_end(X, m);
+          const int ky = b->mol_cls_off[(size_t)Y * nm + m];  // molecule's class-Y list start
+          const int *bk = &b->mol_bkt[((size_t)Y * nm + m) * (kNumBuckets + 1)];
+          const int k0 = ky + bk[kb], k1 = ky + bk[kb + 1];
+          for (int i = b0; i < b1; ++i) {
+            const double qb = b->pairs[i].Q;
+            int lo = k0, hi = k1;  // first ket whose whole Schwarz bin has qb*Q < thrs
+            while (lo < hi) {
+              const int mid = (lo + hi) >> 1;
+              if (qb * q_bin_upper(q_bin(b->pairs[mid].Q)) >= thrs)
+                lo = mid + 1;
+              else
+                hi = mid;
+            }
+            int n = lo - k0;
+            // X == Y: ket position <= bra position inside the molecule's class list
+            if (X == Y) n = std::max(0, std::min(n, (i - b0) - bk[kb] + 1));
+            acc += n;
+            qoff.push_back(acc);
+            kbase.push_back(k0 - b->cls_off[Y]);
           }
-          int n = lo - k0;
-          if (X == Y) n = std::min(n, i - b0 + 1);
-          acc += n;
-          qoff.push_back(acc);
-          kbase.push_back(k0 - b->cls_off[Y]);
+        }
+        bp.nquartet = acc;
+        if (acc > 0)
+          plan.push_back(bp);
+        else {
+          qoff.resize(bp.off);
+          kbase.resize(bp.koff);
         }
       }
-      bp.nquartet = acc;
-      if (acc > 0) plan.push_back(bp);
-    }
   if (b->d_qoff) cudaFree(b->d_qoff);
   if (b->d_kbase) cudaFree(b->d_kbase);
   b->d_qoff = nullptr;
@@ -320,6 +336,7 @@ static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double h
   a.Fh = b->d_Fh;
   a.jscale[0] = 1.0;
   a.kscale[0] = 0.5 * hfx;
+  a.schwarz_thr = b->plan_thrs;  // the plan's last Schwarz bin may reach below the threshold
   int slot = 0;
   for (const BatchPlan &bp : b->plan) {
     a.bra = b->d_pairs + b->cls_off[bp.X];
@@ -337,8 +354,8 @@ static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double h
     const int lc = (bp.Y == 0) ? 0 : (bp.Y <= 2) ? 1 : (bp.Y <= 5) ? 2 : 3;
     const int ld = bp.Y - lc * (lc + 1) / 2;
     a.boys = b->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-    const ClassKernel *kp = &jk_kernel_variant(bp.X, bp.Y, 0, b->choice[bp.X][bp.Y]);
-    if (!kp->launch) kp = &jk_kernel(bp.X, bp.Y, 0);
+    const ClassKernel *kp = &jk_kernel_variant(bp.X, bp.Y, 0, b->choice[bp.X][bp.Y], bp.bucket == 0);
+    if (!kp->launch) kp = &jk_kernel(bp.X, bp.Y, 0, bp.bucket == 0);
     const ClassKernel &k = *kp;
     const int64_t per_block = (k.smem == 0) ? k.block : 1;
     const int grid = (int)std::max<int64_t>(
@@ -415,8 +432,7 @@ extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, do
     unsigned long long s[4] = {0, 0, 0, 0};
     for (int i = 0; i < kCounterSlots; ++i)
       for (int k = 0; k < 4; ++k) s[k] += cnt[4 * i + k];
-    int64_t tq = 0;
-    for (const BatchPlan &bp : b->plan) tq += bp.nquartet;
+    const int64_t tq = (int64_t)(s[0] + s[2]);  // quartets that passed Schwarz
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     stats->quartets_total = tq;

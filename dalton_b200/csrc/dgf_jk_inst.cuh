@@ -29,6 +29,14 @@ constexpr bool thread_eligible(int LA, int LB, int LC, int LD) {
   return L <= 5;
 }
 
+// Classes with f shells up to L = 5 get the thread kernel in its
+// single-ket-primitive form only (every pair of a Dunning basis in the
+// working basis has one primitive pair), first chunk variant; their other
+// plan entries keep the team kernel.
+constexpr bool k1_only_eligible(int LA, int LB, int LC, int LD) {
+  return !thread_eligible(LA, LB, LC, LD) && LA + LB + LC + LD <= 5;
+}
+
 constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 constexpr int cmin(int a, int b) { return a < b ? a : b; }
 // A-chunk count keeping at most `target` accumulators per thread.
@@ -46,10 +54,50 @@ void launch_thread(const JKArgs &a, int grid, int block, size_t smem, cudaStream
   jk_thread_kernel<LA, LB, LC, LD, T, CA, K1><<<dim3(grid, CA), block, smem, s>>>(a);
 }
 
+// Thread-kernel chunk counts of a class: FP64 / FP32, first and second variant.
 template <int LA, int LB, int LC, int LD>
-cudaError_t prepare_team() {
-  return cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)TeamShape<LA, LB, LC, LD>::smem());
+struct ThreadCfg {
+  static constexpr int c64 = chunks_for(LA, LB, LC, LD, 27), c64b = cmin(ncart(LA), 2 * c64);
+  static constexpr int c32 = chunks_for(LA, LB, LC, LD, 54), c32b = cmin(ncart(LA), 2 * c32);
+};
+
+// The thread kernels keep ~10 KB of shared memory per block (Boys and
+// spherical tables, bra Hermite tables): ask for a small shared-memory
+// carveout so that the rest of the unified L1 caches the density rows and
+// pair records their quartets gather.
+constexpr int kThreadCarveoutPercent = 25;
+
+template <int LA, int LB, int LC, int LD, typename T, int CA, int K1>
+cudaError_t carve_one() {
+  return cudaFuncSetAttribute(jk_thread_kernel<LA, LB, LC, LD, T, CA, K1>,
+                              cudaFuncAttributePreferredSharedMemoryCarveout, kThreadCarveoutPercent);
+}
+
+template <int LA, int LB, int LC, int LD, typename T, int CA>
+cudaError_t carve_thread() {
+  cudaError_t e = carve_one<LA, LB, LC, LD, T, CA, 0>();
+  if (e == cudaSuccess) e = carve_one<LA, LB, LC, LD, T, CA, 1>();
+  return e;
+}
+
+template <int LA, int LB, int LC, int LD>
+cudaError_t prepare_class() {
+  cudaError_t e = cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TeamShape<LA, LB, LC, LD>::smem());
+  if constexpr (thread_eligible(LA, LB, LC, LD)) {
+    using C = ThreadCfg<LA, LB, LC, LD>;
+    if (e == cudaSuccess) e = carve_thread<LA, LB, LC, LD, double, C::c64>();
+    if (e == cudaSuccess) e = carve_thread<LA, LB, LC, LD, float, C::c32>();
+    if constexpr (C::c64b != C::c64)
+      if (e == cudaSuccess) e = carve_thread<LA, LB, LC, LD, double, C::c64b>();
+    if constexpr (C::c32b != C::c32)
+      if (e == cudaSuccess) e = carve_thread<LA, LB, LC, LD, float, C::c32b>();
+  } else if constexpr (k1_only_eligible(LA, LB, LC, LD)) {
+    using C = ThreadCfg<LA, LB, LC, LD>;
+    if (e == cudaSuccess) e = carve_one<LA, LB, LC, LD, double, C::c64, 1>();
+    if (e == cudaSuccess) e = carve_one<LA, LB, LC, LD, float, C::c32, 1>();
+  }
+  return e;
 }
 
 template <int LA, int LB, int LC, int LD, typename T, int CA, int K1 = 0>
@@ -65,12 +113,12 @@ void fill_one() {
   constexpr int block = work >= 512 ? 128 : work >= 64 ? 64 : 32;
   JKEntry &e = g_jk_table[X][Y];
   e.team = ClassKernel{&launch_team<LA, LB, LC, LD>, block, S::smem(), 1};
-  e.prepare = &prepare_team<LA, LB, LC, LD>;
+  e.prepare = &prepare_class<LA, LB, LC, LD>;
   for (int p = 0; p < 2; ++p)
     for (int v = 0; v < kThreadVariants; ++v) e.thr[p][v] = e.thr1[p][v] = ClassKernel{nullptr, 0, 0, 0};
   if constexpr (thread_eligible(LA, LB, LC, LD)) {
-    constexpr int c64 = chunks_for(LA, LB, LC, LD, 27), c64b = cmin(ncart(LA), 2 * c64);
-    constexpr int c32 = chunks_for(LA, LB, LC, LD, 54), c32b = cmin(ncart(LA), 2 * c32);
+    using C = ThreadCfg<LA, LB, LC, LD>;
+    constexpr int c64 = C::c64, c64b = C::c64b, c32 = C::c32, c32b = C::c32b;
     e.thr[0][0] = thread_entry<LA, LB, LC, LD, double, c64>();
     e.thr[1][0] = thread_entry<LA, LB, LC, LD, float, c32>();
     if constexpr (c64b != c64) e.thr[0][1] = thread_entry<LA, LB, LC, LD, double, c64b>();
@@ -79,6 +127,10 @@ void fill_one() {
     e.thr1[1][0] = thread_entry<LA, LB, LC, LD, float, c32, 1>();
     if constexpr (c64b != c64) e.thr1[0][1] = thread_entry<LA, LB, LC, LD, double, c64b, 1>();
     if constexpr (c32b != c32) e.thr1[1][1] = thread_entry<LA, LB, LC, LD, float, c32b, 1>();
+  } else if constexpr (k1_only_eligible(LA, LB, LC, LD)) {
+    using C = ThreadCfg<LA, LB, LC, LD>;
+    e.thr1[0][0] = thread_entry<LA, LB, LC, LD, double, C::c64, 1>();
+    e.thr1[1][0] = thread_entry<LA, LB, LC, LD, float, C::c32, 1>();
   }
 }
 

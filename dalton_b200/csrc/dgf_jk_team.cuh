@@ -98,19 +98,34 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
   const int FC = nfun(LC, a.spherical), FD = nfun(LD, a.spherical);
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
 
-  for (int64_t q = a.q_begin + blockIdx.x; q < a.nquartet; q += gridDim.x) {
+  // One contiguous range of the queue per block: thread 0 finds its first
+  // bra once and then walks forward along the prefix sums.
+  const int64_t span = (a.nquartet - a.q_begin + gridDim.x - 1) / gridDim.x;
+  const int64_t qbeg = a.q_begin + (int64_t)blockIdx.x * span, qend = min(qbeg + span, a.nquartet);
+  int ibw = -1;
+  for (int64_t q = qbeg; q < qend; ++q) {
     __syncthreads();
     if (tid == 0) {
       int ib, ic;
       if (a.diag_out) {
         ib = ic = (int)q;
       } else {
-        ib = find_bra(a.qoff, a.nbra, q);
+        if (ibw < 0) {
+          ibw = find_bra(a.qoff, a.nbra, q);
+        } else {
+          int steps = 0;
+          while (q >= a.qoff[ibw + 1] && steps < 32) {
+            ++ibw;
+            ++steps;
+          }
+          if (q >= a.qoff[ibw + 1]) ibw = find_bra(a.qoff, a.nbra, q);
+        }
+        ib = ibw;
         ic = (int)(q - a.qoff[ib]) + (a.kbase ? a.kbase[ib] : 0);
       }
       s_ib = ib;
       s_ic = ic;
-      const PairRec &br = a.bra[ib], &kt = a.ket[ic];
+      const PairRec br = load_pair(a.bra + ib), kt = load_pair(a.ket + ic);
       s_sel = a.diag_out ? 0 : quartet_select(a, br, kt);
       double w = 1.0;
       if (br.same) w *= 0.5;
@@ -123,7 +138,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
       if (tid == 0 && s_sel == 2) ++cnt_s;
       continue;
     }
-    const PairRec br = a.bra[s_ib], kt = a.ket[s_ic];
+    const PairRec br = load_pair(a.bra + s_ib), kt = load_pair(a.ket + s_ic);
     for (int e = tid; e < NAB * NCD; e += nt) out[e] = 0.0;
     for (int i = 0; i < br.npp; ++i) {
       const PrimPair P1 = a.pp[br.pp0 + i];
