@@ -469,11 +469,11 @@ def main():
     peak = fp64_peak if top["precision"] == 64 else fp32_peak
     tot_ms = sum(r["ms"] for r in prof)
     roofline = {"bound": "fp64" if top["precision"] == 64 else "fp32",
-                "kernel": f"jk_{'thread' if top['kernel'] == 0 else 'team'}_kernel<{top['la']},{top['lb']},"
+                "kernel": f"jk_{('thread', 'team', 'team')[top['kernel']]}_kernel<{top['la']},{top['lb']},"
                           f"{top['lc']},{top['ld']},{'double' if top['precision'] == 64 else 'float'}>",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": "measured FMA-loop peak on this GPU (MEASURED_PEAKS.json has no FP64 figure)",
-                "traffic": ncu_traffic(f"jk_{'thread' if top['kernel'] == 0 else 'team'}_kernel<{top['la']},{top['lb']},"
+                "traffic": ncu_traffic(f"jk_{('thread', 'team', 'team')[top['kernel']]}_kernel<{top['la']},{top['lb']},"
                                        f"{top['lc']},{top['ld']},{'double' if top['precision'] == 64 else 'float'}>",
                                        args.workload),
                 "share_of_build": top["ms"] / tot_ms if tot_ms else None,

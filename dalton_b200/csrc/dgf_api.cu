@@ -219,7 +219,7 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
                          int precision) {
   if (!k.launch) DGF_FAIL(DGF_ERR_UNSUPPORTED, "no kernel for this class and precision");
   const bool thread_kernel = (k.smem == 0);
-  const int64_t per_block = thread_kernel ? k.block : 1;  // thread kernels: a quartet per thread
+  const int64_t per_block = k.qpb;  // thread kernels: a quartet per thread; team kernels: per block or per warp
   const int64_t nq = args.nquartet - args.q_begin;
   if (nq <= 0 && !args.diag_out) return DGF_OK;
   int64_t grid64 = std::min<int64_t>((nq + per_block - 1) / per_block, (int64_t)c->nsm * 16);
@@ -243,7 +243,7 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
     r.lc = cls_l1(Y);
     r.ld = Y - r.lc * (r.lc + 1) / 2;
     r.precision = (precision == 1) ? 32 : 64;
-    r.kernel = thread_kernel ? 0 : 1;
+    r.kernel = thread_kernel ? 0 : (k.qpb > 1 ? 2 : 1);
     (void)k;
     r.quartets = args.nquartet - args.q_begin;
     r.evaluated = 0;
@@ -1178,7 +1178,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
       float best = 1e30f;
       int bestv = c->choice[cp.X][cp.Y][p];
       a.boys = c->d_boys + (p ? boys_low_offset(la + lb + lc + ld) : (size_t)(la + lb + lc + ld) * kBoysTableDoubles);
-      for (int v = -1; v < kThreadVariants; ++v) {
+      for (int v = -2; v < kThreadVariants; ++v) {
         if (!jk_kernel_variant(cp.X, cp.Y, p, v).launch && !jk_kernel_variant(cp.X, cp.Y, p, v, true).launch)
           continue;
         int chunks = 1;

@@ -357,7 +357,7 @@ static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double h
     const ClassKernel *kp = &jk_kernel_variant(bp.X, bp.Y, 0, b->choice[bp.X][bp.Y], bp.bucket == 0);
     if (!kp->launch) kp = &jk_kernel(bp.X, bp.Y, 0, bp.bucket == 0);
     const ClassKernel &k = *kp;
-    const int64_t per_block = (k.smem == 0) ? k.block : 1;
+    const int64_t per_block = k.qpb;
     const int grid = (int)std::max<int64_t>(
         1, std::min<int64_t>((bp.nquartet + per_block - 1) / per_block, (int64_t)b->nsm * 16));
     k.launch(a, grid, k.block, k.smem, st);

@@ -143,6 +143,7 @@ struct ClassKernel {
   int block;
   size_t smem;   // dynamic shared memory (team kernels); 0 for thread kernels
   int chunks;    // thread kernels: A-component chunks (grid.y)
+  int qpb;       // quartets a block works on at a time (grid sizing)
 };
 
 constexpr int kThreadVariants = 2;
@@ -152,7 +153,8 @@ constexpr int kThreadVariants = 2;
 // ket1: the launch's kets have one primitive pair each (thread kernels then
 // use their single-ket-primitive form).
 const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1 = false);
-// variant -1 = team kernel, >= 0 = thread-kernel variant (precision 0/1).
+// variant -2 = warp-team kernel, -1 = team kernel, >= 0 = thread-kernel
+// variant (precision 0/1).
 const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1 = false);
 cudaError_t jk_prepare_all();
 

@@ -10,13 +10,14 @@ namespace dgf {
 JKEntry g_jk_table[kNumPairClass][kNumPairClass];
 
 namespace {
-const ClassKernel kNone{nullptr, 0, 0, 0};
+const ClassKernel kNone{nullptr, 0, 0, 0, 0};
 }
 
-// variant: -1 = team kernel, 0.. = thread-kernel variant; precision 0 = FP64,
+// variant: -2 = warp-team kernel, -1 = team kernel, 0.. = thread-kernel variant; precision 0 = FP64,
 // 1 = FP32.  Returns a kernel with launch == nullptr when absent.
 const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1) {
   const JKEntry &e = g_jk_table[X][Y];
+  if (variant == -2) return precision == 0 ? e.wteam : kNone;
   if (variant < 0) return precision == 0 ? e.team : kNone;
   if (variant >= kThreadVariants) return kNone;
   const int p = precision ? 1 : 0;

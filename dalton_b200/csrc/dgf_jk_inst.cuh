@@ -11,6 +11,7 @@ namespace dgf {
 
 struct JKEntry {
   ClassKernel team;
+  ClassKernel wteam;                     // one quartet per warp (light quartets), when it fits
   ClassKernel thr[2][kThreadVariants];   // [precision 0 = FP64, 1 = FP32][variant]
   ClassKernel thr1[2][kThreadVariants];  // same, for kets of one primitive pair each
   cudaError_t (*prepare)();
@@ -44,9 +45,9 @@ constexpr int chunks_for(int LA, int LB, int LC, int LD, int target) {
   return cmin(ncart(LA), cdiv(ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD), target));
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, int WT>
 void launch_team(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
-  jk_team_kernel<LA, LB, LC, LD><<<grid, block, smem, s>>>(a);
+  jk_team_kernel<LA, LB, LC, LD, WT><<<grid, block, smem, s>>>(a);
 }
 
 template <int LA, int LB, int LC, int LD, typename T, int CA, int K1>
@@ -82,8 +83,13 @@ cudaError_t carve_thread() {
 
 template <int LA, int LB, int LC, int LD>
 cudaError_t prepare_class() {
-  cudaError_t e = cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TeamShape<LA, LB, LC, LD>::smem());
+  using TS = TeamShape<LA, LB, LC, LD>;
+  cudaError_t e = cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TS::smem());
+  if constexpr (TS::kWarpTeams > 0)
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD, TS::kWarpTeams>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::smem_w(TS::kWarpTeams));
   if constexpr (thread_eligible(LA, LB, LC, LD)) {
     using C = ThreadCfg<LA, LB, LC, LD>;
     if (e == cudaSuccess) e = carve_thread<LA, LB, LC, LD, double, C::c64>();
@@ -102,7 +108,7 @@ cudaError_t prepare_class() {
 
 template <int LA, int LB, int LC, int LD, typename T, int CA, int K1 = 0>
 ClassKernel thread_entry() {
-  return ClassKernel{&launch_thread<LA, LB, LC, LD, T, CA, K1>, kThreadBlock, 0, CA};
+  return ClassKernel{&launch_thread<LA, LB, LC, LD, T, CA, K1>, kThreadBlock, 0, CA, kThreadBlock};
 }
 
 template <int X, int Y>
@@ -112,10 +118,15 @@ void fill_one() {
   constexpr int work = S::NAB * S::NCD;
   constexpr int block = work >= 512 ? 128 : work >= 64 ? 64 : 32;
   JKEntry &e = g_jk_table[X][Y];
-  e.team = ClassKernel{&launch_team<LA, LB, LC, LD>, block, S::smem(), 1};
+  e.team = ClassKernel{&launch_team<LA, LB, LC, LD, 0>, block, S::smem(), 1, 1};
+  if constexpr (S::kWarpTeams > 0)
+    e.wteam = ClassKernel{&launch_team<LA, LB, LC, LD, S::kWarpTeams>, 32 * S::kWarpTeams,
+                          S::smem_w(S::kWarpTeams), 1, S::kWarpTeams};
+  else
+    e.wteam = ClassKernel{nullptr, 0, 0, 0, 0};
   e.prepare = &prepare_class<LA, LB, LC, LD>;
   for (int p = 0; p < 2; ++p)
-    for (int v = 0; v < kThreadVariants; ++v) e.thr[p][v] = e.thr1[p][v] = ClassKernel{nullptr, 0, 0, 0};
+    for (int v = 0; v < kThreadVariants; ++v) e.thr[p][v] = e.thr1[p][v] = ClassKernel{nullptr, 0, 0, 0, 0};
   if constexpr (thread_eligible(LA, LB, LC, LD)) {
     using C = ThreadCfg<LA, LB, LC, LD>;
     constexpr int c64 = C::c64, c64b = C::c64b, c32 = C::c32, c32b = C::c32b;

@@ -47,8 +47,16 @@ struct TeamShape {
   static constexpr int EA = (LA + 1) * (LB + 1) * (LAB + 1), EC = (LC + 1) * (LD + 1) * (LCD + 1);
   static constexpr int XS = cmax(N3AB * NCD, NAB * NCD);
   static constexpr int DST = 6 * 100;  // six density blocks of up to 10x10 (Cartesian f)
-  static constexpr int NDOUBLE = kBoysTableDoubles + 2 * N3L + 3 * EA + 3 * EC + XS + NAB * NCD + DST + kSphTableDoubles;
-  static constexpr size_t smem() { return (size_t)NDOUBLE * 8 + (size_t)N3L * 4; }
+  // per quartet in flight: R ping-pong, Hermite tables, half-transformed and
+  // final blocks, density blocks, and the scalars (F_n, P-Q, weight)
+  static constexpr int PQ = 2 * N3L + 3 * EA + 3 * EC + XS + NAB * NCD + DST + (L + 1) + 4;
+  // shared by the block: Boys and spherical tables, packed (t,u,v) of R
+  static constexpr size_t smem_w(int nq) {
+    return ((size_t)kBoysTableDoubles + kSphTableDoubles + (size_t)nq * PQ) * 8 + (size_t)N3L * 4;
+  }
+  static constexpr size_t smem() { return smem_w(1); }
+  // warp teams (one quartet per warp) per block, 0 when four or two do not fit in 96 KB
+  static constexpr int kWarpTeams = smem_w(4) <= 96 * 1024 ? 4 : smem_w(2) <= 96 * 1024 ? 2 : 0;
 };
 
 // One step of the Cartesian->spherical transform of index k of a 4-index block.
@@ -64,47 +72,63 @@ __device__ __forceinline__ void sph_step(const double *in, double *outb, int pre
   }
 }
 
-template <int LA, int LB, int LC, int LD>
+// WT = 0: the whole block works on one quartet at a time.  WT > 0: each of
+// the block's WT warps works on its own quartet (its own slice of shared
+// memory, warp-level synchronisation), which keeps several light quartets
+// (single primitive pairs) in flight per block instead of one.
+template <int LA, int LB, int LC, int LD, int WT = 0>
 __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
   using S = TeamShape<LA, LB, LC, LD>;
   constexpr int L = S::L, LAB = S::LAB, LCD = S::LCD;
   constexpr int NB = S::NB, ND = S::ND, NAB = S::NAB, NCD = S::NCD;
   constexpr int N3L = S::N3L, N3AB = S::N3AB, EA = S::EA, EC = S::EC;
+  constexpr int NQ = WT ? WT : 1;
   extern __shared__ double sm[];
+  const int sub = WT ? (int)(threadIdx.x >> 5) : 0;
   double *tab = sm;
-  double *Ra = tab + kBoysTableDoubles;
+  double *sph = tab + kBoysTableDoubles;
+  double *Ra = sph + kSphTableDoubles + (size_t)sub * S::PQ;
   double *Rb = Ra + N3L;
   double *eab = Rb + N3L;
   double *ecd = eab + 3 * EA;
   double *X = ecd + 3 * EC;
   double *out = X + S::XS;
   double *dst = out + NAB * NCD;
-  double *sph = dst + S::DST;
-  int *tuvt = (int *)(sph + kSphTableDoubles);
-  __shared__ double sF[L + 1];
-  __shared__ double sPQ[3];
-  __shared__ int s_ib, s_ic, s_sel;
-  __shared__ double s_w, s_red[4];
+  double *sF = dst + S::DST;
+  double *sPQ = sF + (L + 1);
+  double &s_w = sPQ[3];
+  int *tuvt = (int *)(sph + kSphTableDoubles + (size_t)NQ * S::PQ);
+  __shared__ int s_int[NQ][3];
+  int &s_ib = s_int[sub][0], &s_ic = s_int[sub][1], &s_sel = s_int[sub][2];
 
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int i = tid; i < kBoysTableDoubles; i += nt) tab[i] = a.boys[i];
-  for (int i = tid; i < kSphTableDoubles; i += nt) sph[i] = a.sph[i];
-  for (int e = tid; e < N3L; e += nt) {
+  for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
+  for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
+  for (int e = threadIdx.x; e < N3L; e += blockDim.x) {
     int t, u, v;
     tuv_decode(e, t, u, v);
     tuvt[e] = t | (u << 8) | (v << 16);
   }
+  __syncthreads();
+  const int tid = WT ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
+  const int nt = WT ? 32 : (int)blockDim.x;
+  auto team_sync = [&]() {
+    if constexpr (WT != 0)
+      __syncwarp();
+    else
+      __syncthreads();
+  };
   const int FA = nfun(LA, a.spherical), FB = nfun(LB, a.spherical);
   const int FC = nfun(LC, a.spherical), FD = nfun(LD, a.spherical);
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
 
-  // One contiguous range of the queue per block: thread 0 finds its first
+  // One contiguous range of the queue per team: its thread 0 finds the first
   // bra once and then walks forward along the prefix sums.
-  const int64_t span = (a.nquartet - a.q_begin + gridDim.x - 1) / gridDim.x;
-  const int64_t qbeg = a.q_begin + (int64_t)blockIdx.x * span, qend = min(qbeg + span, a.nquartet);
+  const int64_t nteam = (int64_t)gridDim.x * NQ, team = (int64_t)blockIdx.x * NQ + sub;
+  const int64_t span = (a.nquartet - a.q_begin + nteam - 1) / nteam;
+  const int64_t qbeg = a.q_begin + team * span, qend = min(qbeg + span, a.nquartet);
   int ibw = -1;
   for (int64_t q = qbeg; q < qend; ++q) {
-    __syncthreads();
+    team_sync();
     if (tid == 0) {
       int ib, ic;
       if (a.diag_out) {
@@ -133,7 +157,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
       if (a.same_class && ib == ic + a.ket_off) w *= 0.5;
       s_w = w;
     }
-    __syncthreads();
+    team_sync();
     if (s_sel) {
       if (tid == 0 && s_sel == 2) ++cnt_s;
       continue;
@@ -171,10 +195,10 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
           sPQ[1] = y;
           sPQ[2] = z;
         }
-        __syncthreads();
+        team_sync();
         double *prev = Ra;
         if (tid == 0) prev[0] = sF[L];
-        __syncthreads();
+        team_sync();
         const double px = sPQ[0], py = sPQ[1], pz = sPQ[2];
         for (int n = L - 1; n >= 0; --n) {
           double *cur = (prev == Ra) ? Rb : Ra;
@@ -199,7 +223,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
             }
             cur[e] = val;
           }
-          __syncthreads();
+          team_sync();
           prev = cur;
         }
         const double *R = prev;
@@ -222,7 +246,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
             }
           X[e] += s;
         }
-        __syncthreads();
+        team_sync();
       }
       for (int e = tid; e < NAB * NCD; e += nt) {
         const int ab = e / NCD, cd = e - ab * NCD;
@@ -241,7 +265,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
           }
         out[e] += s;
       }
-      __syncthreads();
+      team_sync();
     }
     cnt_q += 1;
     cnt_p += (unsigned long long)br.npp * kt.npp;
@@ -257,7 +281,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
         for (int m = 0; m < k; ++m) pre *= dims[m];
         for (int m = k + 1; m < 4; ++m) post *= dims[m];
         sph_step(res, tmp, pre, dims[k], 2 * ls[k] + 1, post, sph + sph_offset(ls[k]), tid, nt);
-        __syncthreads();
+        team_sync();
         dims[k] = 2 * ls[k] + 1;
         double *sw = res;
         res = tmp;
@@ -294,7 +318,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
         if (r < FA && c < FD) Dad[r * FD + c] = Dk[(size_t)(aoA + r) * N + aoD + c];
         if (r < FA && c < FC) Dac[r * FC + c] = Dk[(size_t)(aoA + r) * N + aoC + c];
       }
-      __syncthreads();
+      team_sync();
       const int FCD = FC * FD, FAB = FA * FB;
       if (js != 0.0) {
         for (int e = tid; e < FAB; e += nt) {
@@ -340,7 +364,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
           atomicAdd(Fk + (size_t)(aoB + b) * N + aoD + d, ks * s);
         }
       }
-      __syncthreads();
+      team_sync();
     }
   }
   if (tid == 0 && a.counters) {
@@ -348,7 +372,6 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
     atomicAdd(a.counters + 1, cnt_p);
     atomicAdd(a.counters + 2, cnt_s);
   }
-  (void)s_red;
 }
 
 }  // namespace dgf

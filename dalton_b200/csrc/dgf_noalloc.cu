@@ -128,7 +128,7 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
     a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
     const ClassKernel *k = &jk_kernel_variant(cp.X, cp.Y, 0, c->choice[cp.X][cp.Y][0], cp.bucket == 0);
     if (!k->launch) k = &jk_kernel(cp.X, cp.Y, 0, cp.bucket == 0);
-    const int64_t per_block = (k->smem == 0) ? k->block : 1;
+    const int64_t per_block = k->qpb;
     const int grid =
         (int)std::max<int64_t>(1, std::min<int64_t>((cp.nquartet + per_block - 1) / per_block, (int64_t)c->nsm * 16));
     k->launch(a, grid, k->block, k->smem, st);

@@ -183,7 +183,7 @@ int dgf_grad1e(dgf_ctx *ctx, const double *dmat, const double *wmat, double *gra
 typedef struct {
   int32_t la, lb, lc, ld;   /* angular momenta of the class (ab|cd) */
   int32_t precision;        /* 64 = FP64, 32 = FP32 contraction */
-  int32_t kernel;           /* 0 = thread-per-quartet, 1 = cooperative team */
+  int32_t kernel;           /* 0 = thread-per-quartet, 1 = cooperative team, 2 = warp teams */
   int64_t quartets;         /* quartets of the class in the plan */
   int64_t evaluated;        /* quartets this launch evaluated */
   int64_t prim_quartets;    /* primitive quartets this launch evaluated */
