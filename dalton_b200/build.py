@@ -1,8 +1,9 @@
 """Build libdgfock.so (the CUDA kernels and the C ABI) for sm_100a, in-tree.
 
-Each ``csrc/*.cu`` file is compiled to an object in parallel, then linked
-into ``dalton_b200/libdgfock.so``.  Objects are rebuilt only when a source or
-header is newer.
+Each ``csrc/*.cu`` file, and one generated unit per quartet-class pair of
+the Fock and gradient kernel tables, is compiled to an object in parallel,
+then linked into ``dalton_b200/libdgfock.so``.  Objects are rebuilt only when
+a source or header is newer.
 """
 from __future__ import annotations
 
@@ -61,9 +62,38 @@ def _compile(src, extra):
     return obj, r.stderr
 
 
+NUM_PAIR_CLASS = 10  # (la >= lb) shell-pair classes up to f
+NUM_GRAD_CLASS = 6   # the gradient covers s, p and d
+
+
+def _class_l(x):
+    la = 0 if x == 0 else 1 if x <= 2 else 2 if x <= 5 else 3
+    return la + (x - la * (la + 1) // 2)
+
+
+def _generated_units():
+    """One translation unit per class pair of the Fock and gradient kernel
+    tables (their templates live in headers), written to the build folder
+    only when the content changes; heaviest classes first."""
+    gen = os.path.join(BUILD, "gen")
+    os.makedirs(gen, exist_ok=True)
+    units = []
+    for kind, header, macro, n in (("jk", "dgf_jk_inst.cuh", "DGF_JK_CLASS", NUM_PAIR_CLASS),
+                                   ("grad", "dgf_grad_kernel.cuh", "DGF_GRAD_CLASS", NUM_GRAD_CLASS)):
+        for x in range(n):
+            for y in range(x + 1):
+                path = os.path.join(gen, f"dgf_{kind}_{x}_{y}.cu")
+                text = f'#include "{header}"\n\n{macro}({x}, {y})\n'
+                if not os.path.exists(path) or open(path).read() != text:
+                    with open(path, "w") as f:
+                        f.write(text)
+                units.append((_class_l(x) + _class_l(y), path))
+    return [p for _, p in sorted(units, key=lambda u: -u[0])]
+
+
 def build(verbose: bool = False, extra=None, jobs: int | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    srcs = _generated_units() + sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     extra = list(extra or [])
     with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count()) as ex:
         res = list(ex.map(lambda s: _compile(s, extra), srcs))

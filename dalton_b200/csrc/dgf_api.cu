@@ -349,6 +349,7 @@ static JKArgs base_args(dgf_ctx *c) {
   a.nbf = c->nwf;
   a.nshell = c->nwshell;
   a.slot_stride = (int64_t)c->nwf * c->nwf;
+  a.ket_pp0 = -1;
   return a;
 }
 
@@ -793,6 +794,14 @@ extern "C" int dgf_count_ao_quartets(dgf_ctx *c, double thrs, dgf_int *count) {
 // pairs whose Schwarz bin can reach Q_AB Q_CD >= thrs (a prefix of the
 // bin-sorted ket bucket; the kernels drop the quartets below thrs), and
 // only kets up to the bra itself when X == Y), as prefix sums.
+// First primitive pair of a plan entry's kets when every ket of the entry
+// has one primitive pair (bucket 0): the primitive pairs are stored in pair
+// order, so ket ic's is pp[base + ic]; -1 otherwise.
+static int ket_pp0_of(const dgf_ctx *c, const ClassPlan &cp) {
+  if (cp.bucket != 0 || cp.kb1 <= cp.kb0) return -1;
+  return c->pairs[c->cls_off[cp.Y] + cp.kb0].pp0;
+}
+
 static int build_plan(dgf_ctx *c, double thrs) {
   if (c->plan_thrs == thrs && !c->plan.empty()) return DGF_OK;
   std::vector<int64_t> all;
@@ -999,6 +1008,7 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
       a.bra = c->d_pairs + c->cls_off[cp.X];
       a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
       a.ket_off = cp.kb0;
+      a.ket_pp0 = ket_pp0_of(c, cp);
       a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
       a.same_class = (cp.X == cp.Y);
       a.qoff = c->d_qoff + cp.off;
@@ -1189,6 +1199,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
             const ClassPlan &cq = c->plan[q];
             a.ket = c->d_pairs + c->cls_off[cq.Y] + cq.kb0;
             a.ket_off = cq.kb0;
+            a.ket_pp0 = ket_pp0_of(c, cq);
             a.qoff = c->d_qoff + cq.off;
             a.nquartet = cq.nquartet;
             // entries this candidate has no kernel for run the FP64 default (same for every candidate)
@@ -1225,6 +1236,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
             const ClassPlan &cq = c->plan[q];
             a.ket = c->d_pairs + c->cls_off[cq.Y] + cq.kb0;
             a.ket_off = cq.kb0;
+            a.ket_pp0 = ket_pp0_of(c, cq);
             a.qoff = c->d_qoff + cq.off;
             a.nquartet = cq.nquartet;
             a.dmax = c->d_dmax;

@@ -336,7 +336,8 @@ static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double h
   a.Fh = b->d_Fh;
   a.jscale[0] = 1.0;
   a.kscale[0] = 0.5 * hfx;
-  a.schwarz_thr = b->plan_thrs;  // the plan's last Schwarz bin may reach below the threshold
+  a.schwarz_thr = b->plan_thrs;
+  a.ket_pp0 = -1;  // a molecule's kets are not adjacent to the next molecule's  // the plan's last Schwarz bin may reach below the threshold
   int slot = 0;
   for (const BatchPlan &bp : b->plan) {
     a.bra = b->d_pairs + b->cls_off[bp.X];

@@ -19,8 +19,8 @@
 // formed from Cartesian 2-index blocks with compile-time sizes; the bra sums
 // over (t, u, v) are nested one direction at a time.
 //
-// Host side; the kernels are in dgf_grad_kernel.cuh, instantiated one bra
-// class per translation unit (dgf_grad_row<X>.cu).
+// Host side; the kernels are in dgf_grad_kernel.cuh, instantiated one class
+// pair per translation unit (DGF_GRAD_CLASS, generated by the build).
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -81,6 +81,7 @@ static int grad_impl(dgf_ctx *c, const double *d1, const double *d2, double hfx,
   a.hfx = hfx;
   a.natom = c->natom;
   a.schwarz_thr = thrs;
+  a.ket_pp0 = -1;
   for (const ClassPlan &cp : c->plan) {
     a.bra = c->d_pairs + c->cls_off[cp.X];
     a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;

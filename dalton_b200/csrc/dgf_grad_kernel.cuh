@@ -455,7 +455,7 @@ constexpr int cls_lb(int X) { return X - cls_la(X) * (cls_la(X) + 1) / 2; }
 constexpr int kGradClasses = 6;  // pair classes up to (dd)
 
 typedef void (*GradLauncher)(const JKArgs &, int, int, cudaStream_t);
-extern GradLauncher g_grad_table[kGradClasses][kGradClasses];  // dgf_grad2e.cu; rows filled by dgf_grad_row<X>.cu
+extern GradLauncher g_grad_table[kGradClasses][kGradClasses];  // dgf_grad2e.cu; filled by DGF_GRAD_CLASS units
 
 template <int LA, int LB, int LC, int LD>
 void launch_grad(const JKArgs &a, int grid, int block, cudaStream_t s) {
@@ -466,22 +466,19 @@ void launch_grad(const JKArgs &a, int grid, int block, cudaStream_t s) {
     grad_thread_kernel<LA, LB, LC, LD, false><<<g, block, 0, s>>>(a);
 }
 
-template <int X, int... Ys>
-void fill_grad_row(std::integer_sequence<int, Ys...>) {
-  ((g_grad_table[X][Ys] = &launch_grad<cls_la(X), cls_lb(X), cls_la(Ys), cls_lb(Ys)>), ...);
-}
 
 }  // namespace grad
 }  // namespace dgf
 
-// Defines the static initialiser that fills row X of the gradient table.
-#define DGF_GRAD_ROW(X)                                                                            \
+// Defines the static initialiser that fills entry (X, Y) of the gradient
+// table (one generated translation unit per class pair).
+#define DGF_GRAD_CLASS(X, Y)                                                                       \
   namespace dgf {                                                                                  \
   namespace grad {                                                                                 \
   namespace {                                                                                      \
-  struct GradRowInit##X {                                                                          \
-    GradRowInit##X() { fill_grad_row<X>(std::make_integer_sequence<int, X + 1>{}); }               \
-  } g_grad_row_init_##X;                                                                           \
+  struct GradClassInit_##X##_##Y {                                                                 \
+    GradClassInit_##X##_##Y() { g_grad_table[X][Y] = &launch_grad<cls_la(X), cls_lb(X), cls_la(Y), cls_lb(Y)>; } \
+  } g_grad_class_init_##X##_##Y;                                                                   \
   }                                                                                                \
   }                                                                                                \
   }

@@ -95,6 +95,7 @@ struct JKArgs {
   const int64_t *qoff;      // prefix sums of ket partners per bra (nbra+1), device
   const int *kbase;         // per bra: first ket of its molecule in the ket list (batches), or null
   int ket_off;              // position of ket[0] in its class list (same-class weight compares ib, ic + ket_off)
+  int ket_pp0;              // >= 0: kets of one primitive pair each, ket ic's primitive pair is pp[ket_pp0 + ic]
   int64_t slot_stride;      // elements between density slots in D, Ds, Fh
   int nbra;
   int same_class;           // bra class == ket class (canonical ket <= bra)

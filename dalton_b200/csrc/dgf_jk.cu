@@ -1,8 +1,8 @@
 // Quartet-class kernel table of libdgfock: for every (bra class, ket class)
 // of angular momenta up to f, the cooperative team kernel and, for the
 // classes up to L = 5, register-resident thread kernels in FP64 and FP32,
-// each in two A-chunk variants (the per-class tuning space).  The rows are
-// filled by dgf_jk_row<X>.cu.
+// each in two A-chunk variants (the per-class tuning space).  The entries
+// are filled by one generated translation unit per class pair (DGF_JK_CLASS).
 #include "dgf_jk_inst.cuh"
 
 namespace dgf {

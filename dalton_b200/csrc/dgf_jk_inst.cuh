@@ -1,6 +1,6 @@
-// Instantiation helpers of the quartet-class kernel table: each
-// dgf_jk_row<X>.cu fills row X (bra class X) of the table, so the rows
-// compile in parallel.
+// Instantiation helpers of the quartet-class kernel table: one translation
+// unit per class pair (generated by the build, see DGF_JK_CLASS) fills its
+// entry, so the classes compile in parallel.
 #pragma once
 
 #include <utility>
@@ -145,20 +145,18 @@ void fill_one() {
   }
 }
 
-template <int X, int... Ys>
-void fill_row(std::integer_sequence<int, Ys...>) {
-  (fill_one<X, Ys>(), ...);
-}
 
 }  // namespace jkinst
 }  // namespace dgf
 
-// Defines the static initialiser that fills row X of the table.
-#define DGF_JK_ROW(X)                                                                         \
+// Defines the static initialiser that fills entry (X, Y) of the table; the
+// build compiles one translation unit per class pair, so the classes compile
+// in parallel.
+#define DGF_JK_CLASS(X, Y)                                                                    \
   namespace dgf {                                                                             \
   namespace {                                                                                 \
-  struct RowInit##X {                                                                         \
-    RowInit##X() { jkinst::fill_row<X>(std::make_integer_sequence<int, X + 1>{}); }         \
-  } g_row_init_##X;                                                                           \
+  struct ClassInit_##X##_##Y {                                                                \
+    ClassInit_##X##_##Y() { jkinst::fill_one<X, Y>(); }                                       \
+  } g_class_init_##X##_##Y;                                                                   \
   }                                                                                           \
   }

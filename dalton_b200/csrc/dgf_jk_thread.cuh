@@ -40,7 +40,7 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
   // The warp's bra pair (valid on every lane) for the warp-reduced J_ab block;
   // a quartet's bra and ket belong to one molecule, so its N x N block is
   // the bra's.
-  const PairRec brw = load_pair(a.bra + ib0);
+  const PairRec brw = load_pair_fock(a.bra + ib0);
   const int N = work ? br.nbfm : brw.nbfm;
   const int64_t db = work ? br.dbase : brw.dbase;
   for (int k = 0; k < a.nslot; ++k) {
@@ -183,6 +183,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
     ibw = ib0;
     int ib = ib0, ic = 0, sel = 1;
     PairRec br, kt;
+    PrimPair P2one;  // K1: the ket's only primitive pair, fetched before the bra work
     if (active) {
       int steps = 0;
       while (q >= a.qoff[ib + 1] && steps < 32) {
@@ -191,8 +192,10 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
       }
       if (q >= a.qoff[ib + 1]) ib = find_bra(a.qoff, a.nbra, q);
       ic = (int)(q - a.qoff[ib]) + (a.kbase ? a.kbase[ib] : 0);
-      br = load_pair(a.bra + ib);
-      kt = load_pair(a.ket + ic);
+      br = load_pair_fock(a.bra + ib);
+      kt = load_pair_fock(a.ket + ic);
+      // K1 with a known layout: the ket's primitive pair is fetched alongside its record
+      if (K1 && a.ket_pp0 >= 0) P2one = load_prim<(LC + LD > 0)>(a.pp + a.ket_pp0 + ic);
       sel = quartet_select(a, br, kt);
       if (sel == 2 && CH == 0 && a.mode != 2) ++cnt_s;  // a split class counts its skips in the FP64 launch
     }
@@ -200,8 +203,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
     Tc acc[NACC];
 #pragma unroll
     for (int k = 0; k < NACC; ++k) acc[k] = Tc(0);
-    PrimPair P2one;  // K1: the ket's only primitive pair, fetched before the bra work
-    if (K1 && work) P2one = load_prim<(LC + LD > 0)>(a.pp + kt.pp0);
+    if (K1 && work && a.ket_pp0 < 0) P2one = load_prim<(LC + LD > 0)>(a.pp + kt.pp0);
     // Bra groups: lanes sharing a bra pair run its primitive loop together.
     unsigned pending = __ballot_sync(full, work);
     while (pending) {
@@ -209,7 +211,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
       const int ibl = __shfl_sync(full, ib, leader);
       const bool mine = work && ib == ibl && ((pending >> lane) & 1u);
       pending &= ~__ballot_sync(full, mine);
-      const PairRec brl = load_pair(a.bra + ibl);
+      const PairRec brl = load_pair_fock(a.bra + ibl);
       for (int i = 0; i < brl.npp; ++i) {
         const PrimPair P1 = load_prim<true>(a.pp + brl.pp0 + i);
         __syncwarp();

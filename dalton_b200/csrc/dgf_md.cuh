@@ -130,6 +130,17 @@ __device__ __forceinline__ PairRec load_pair(const PairRec *p) {
   return r;
 }
 
+// The fields of a pair record the Fock kernels read (all but the atoms).
+__device__ __forceinline__ PairRec load_pair_fock(const PairRec *p) {
+  PairRec r;
+  const int4 *s = reinterpret_cast<const int4 *>(p);
+  int4 *d = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) d[k] = __ldg(s + k);
+  d[3] = make_int4(0, 0, 0, 0);
+  return r;
+}
+
 template <bool PAB>
 __device__ __forceinline__ PrimPair load_prim(const PrimPair *p) {
   PrimPair r;

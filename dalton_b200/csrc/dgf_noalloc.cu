@@ -116,6 +116,7 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
     a.bra = c->d_pairs + c->cls_off[cp.X];
     a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
     a.ket_off = cp.kb0;
+    a.ket_pp0 = (cp.bucket == 0 && cp.kb1 > cp.kb0) ? c->pairs[c->cls_off[cp.Y] + cp.kb0].pp0 : -1;
     a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
     a.same_class = (cp.X == cp.Y);
     a.qoff = c->d_qoff + cp.off;
