@@ -216,6 +216,23 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def scf_summary(ref, inc, mix, seconds):
+    """Whole-SCF comparison (converged to |FDS - SDF| < 1e-6): full FP64 builds
+    against incremental builds under the IFTHRS schedule, FP64 and mixed."""
+    if ref is None:
+        return None
+    leg = lambda r: {"energy": r["energy"], "iterations": r["niter"], "fock_ms_total": r["fock_ms"],
+                     "ifthrs": r["ifthrs"]}
+    return {"fp64_full_builds": leg(ref), "fp64_incremental_screened": leg(inc),
+            "mixed_incremental_screened": leg(mix),
+            "energy_diff_mixed_vs_fp64_full_Eh": abs(mix["energy"] - ref["energy"]),
+            "energy_diff_incremental_vs_fp64_full_Eh": abs(inc["energy"] - ref["energy"]),
+            "fock_speedup_mixed_incremental_vs_fp64_full": ref["fock_ms"] / mix["fock_ms"],
+            "fock_speedup_fp64_incremental_vs_fp64_full": ref["fock_ms"] / inc["fock_ms"],
+            "note": "fock_ms_total: synchronised host time of the Fock builds summed over the SCF iterations",
+            "seconds_all": seconds}
+
+
 def ncu_traffic(kernel, workload):
     """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of
     `kernel` on `workload`, as recorded from an ncu capture of the same
@@ -359,18 +376,23 @@ def main():
             pg.all_reduce(F)
         return F
 
-    # Density: 12-iteration RHF with the FP64 builds (replicated on every rank).
-    t0 = time.perf_counter()
+    # Density of the timed builds: 12-iteration RHF with FP64 builds (replicated on every rank).
     scf64 = rhf(bs, fb, maxiter=args.scf_iters, fixed_iterations=args.scf_iters, thrs=THRS)
-    scf_mix = rhf(bs, fb, maxiter=args.scf_iters, fixed_iterations=args.scf_iters, thrs=THRS,
-                  mixed_cutoff=MIXED_CUTOFF)
-    scf_s = time.perf_counter() - t0
     D = scf64["dmat"].contiguous()
     H = scf64["H"]
-    # Per-class kernel choice on this density (FP64 and FP32 candidates).
+    # Per-class kernel choice on this density (FP64 and FP32 candidates, mixed split).
     t0 = time.perf_counter()
     tuning = fb.autotune(D, thrs=THRS, mixed_cutoff=MIXED_CUTOFF)
     tune_s = time.perf_counter() - t0
+    # Whole SCF to |FDS - SDF| < 1e-6 three ways: full FP64 builds (the drop-in), and
+    # incremental difference-density builds under Dalton's IFTHRS schedule, FP64 and mixed.
+    t0 = time.perf_counter()
+    scf_ref = scf_inc = scf_mix = None
+    if world == 1:
+        scf_ref = rhf(bs, fb, conv=1e-6, maxiter=60, thrs=THRS, incremental=False)
+        scf_inc = rhf(bs, fb, conv=1e-6, maxiter=60, thrs=THRS, ifthrs_schedule=True)
+        scf_mix = rhf(bs, fb, conv=1e-6, maxiter=60, thrs=THRS, mixed_cutoff=MIXED_CUTOFF, ifthrs_schedule=True)
+    scf_s = time.perf_counter() - t0
     enuc = scf64["enuc"]
     # Accuracy of the mixed build at the converged density.
     F64 = build(D, False).clone()
@@ -534,9 +556,7 @@ def main():
             "mixed": {"ms": msmx, "quartets_per_s": quartets / (msmx * 1e-3), "quartets": quartets,
                       "working_basis_quartets": qmx,
                       "energy_error_Eh": dE, "max_abs_dF": dF, "speedup_vs_fp64": ms64 / msmx},
-            "scf": {"iterations": args.scf_iters, "energy_fp64": scf64["energy"], "energy_mixed_incremental":
-                    scf_mix["energy"], "energy_diff_Eh": abs(scf_mix["energy"] - scf64["energy"]),
-                    "seconds_both": scf_s},
+            "scf": scf_summary(scf_ref, scf_inc, scf_mix, scf_s),
             "e2e": {"value": quartets / (e2e_ms * 1e-3), "unit": "quartets/s", "ms": e2e_ms,
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
             "roofline": roofline, "build_tflops_model": build_tflops,

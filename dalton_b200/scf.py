@@ -9,6 +9,12 @@ build (``DIIS_CTL``, DALTON/sirius/sirdiis.F:282):
 * incremental difference-density Fock builds: ``G(D_n) = G(D_{n-1}) +
   G(D_n - D_{n-1})`` (DIFDEN, sirdiis.F:551-567, 733-773, 811-825), with a
   full rebuild every ``full_every`` iterations;
+* optionally Dalton's integral-screening schedule for direct SCF
+  (``ifthrs_schedule``, sirdiis.F:520-523, 1224-1248): the density screen
+  Q_AB Q_CD |D| < 10^-IFTHRS is loose while the orbital gradient is large
+  and tightens with it, IFTHRS = -log10(|g| / SCRFAC) + 3 clamped to
+  [IFTMIN, IFTMAX], SCRFAC = 100 N^2; a tightened threshold forces a full
+  build, otherwise the build is incremental;
 * DIIS extrapolation on the orbital gradient ``FDS - SDF``;
 * energy ``E = 1/2 sum D (H + F) + E_nuc`` (EMY, sirdiis.F:825).
 
@@ -30,7 +36,8 @@ from .fock import FockBuilder
 
 def rhf(bs: BasisSet, fb: FockBuilder | None = None, conv: float = 1e-8, maxiter: int = 50, thrs: float = 1e-12,
         mixed_cutoff: float = 0.0, incremental: bool = True, full_every: int = 8, diis_size: int = 8,
-        device: str = "cuda", verbose: bool = False, fixed_iterations: int | None = None):
+        device: str = "cuda", verbose: bool = False, fixed_iterations: int | None = None,
+        ifthrs_schedule: bool = False):
     """Run RHF; returns a dict with energy, density, orbitals, timings."""
     import torch
 
@@ -58,14 +65,22 @@ def rhf(bs: BasisSet, fb: FockBuilder | None = None, conv: float = 1e-8, maxiter
     fock_ms = 0.0
     nbuild = 0
     it = 0
+    # Dalton's screening limits (sirdiis.F:520-523), conv playing THDIIS
+    scrfac = 100.0 * bs.nbf * bs.nbf
+    iftmax = int(-np.log10(conv / scrfac)) + 1
+    iftmin = int(-np.log10(0.1 / scrfac)) + 1
+    ifthrs = iftmin if ifthrs_schedule else 20
+    newthr = False
+    ifthrs_used = []
     for it in range(1, maxiter + 1):
-        full = (not incremental) or G_prev is None or (it % full_every == 0)
+        full = (not incremental) or G_prev is None or (it % full_every == 0) or newthr
         t0 = time.perf_counter()
         if full:
-            G = fb.herfck_device(D, ifctyp=13, thrs=thrs, mixed_cutoff=mixed_cutoff)
+            G = fb.herfck_device(D, ifctyp=13, thrs=thrs, ifthrs=ifthrs, mixed_cutoff=mixed_cutoff)
         else:
-            dG = fb.herfck_device(D - D_prev, ifctyp=13, thrs=thrs, mixed_cutoff=mixed_cutoff)
+            dG = fb.herfck_device(D - D_prev, ifctyp=13, thrs=thrs, ifthrs=ifthrs, mixed_cutoff=mixed_cutoff)
             G = G_prev + dG
+        ifthrs_used.append(ifthrs)
         torch.cuda.synchronize(dev)
         fock_ms += (time.perf_counter() - t0) * 1e3
         nbuild += 1
@@ -75,6 +90,13 @@ def rhf(bs: BasisSet, fb: FockBuilder | None = None, conv: float = 1e-8, maxiter
         err = X.T @ (F @ D @ S - S @ D @ F) @ X
         en = float(torch.linalg.norm(err))
         history.append((energy, en, bool(full)))
+        if ifthrs_schedule:  # next build's screening threshold (sirdiis.F:1224-1248, DIFDEN form)
+            ithrs = int(-np.log10(max(en, 1e-300) / scrfac)) + 3
+            if ithrs >= iftmax - 2:
+                ithrs = iftmax
+            newthr = abs(ithrs - ifthrs) >= 2
+            if newthr:
+                ifthrs = min(iftmax, max(iftmin, ithrs))
         if verbose:
             print(f"iter {it:3d}  E = {energy:.12f}  |g| = {en:.3e}  {'full' if full else 'incr'}")
         if fixed_iterations is None and en < conv:
@@ -102,7 +124,7 @@ def rhf(bs: BasisSet, fb: FockBuilder | None = None, conv: float = 1e-8, maxiter
     Cocc = C[:, :nocc]
     W = 2.0 * (Cocc * eps[:nocc]) @ Cocc.T
     return dict(energy=energy, dmat=D, C=C, eps=eps, wmat=W, S=S, H=H, fock=F, niter=it, nocc=nocc, enuc=enuc,
-                history=history, fock_ms=fock_ms, nbuild=nbuild, builder=fb)
+                history=history, fock_ms=fock_ms, nbuild=nbuild, builder=fb, ifthrs=ifthrs_used)
 
 
 def energy_of(D, H, G, enuc: float) -> float:

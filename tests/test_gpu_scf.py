@@ -76,6 +76,22 @@ def test_mixed_precision_accuracy(cuda, orc):
     assert np.abs(f64.cpu().numpy() - ref).max() < 1e-10
 
 
+def test_ifthrs_schedule_scf_energy(cuda):
+    """Dalton's direct-SCF screening schedule (loose while the orbital
+    gradient is large, tight near convergence) with incremental and mixed
+    builds reaches the energy of plain full FP64 builds."""
+    from dalton_b200.scf import rhf
+
+    bs = build_basis(molecules.water_cluster(4, (2, 2, 1), seed=1), "cc-pVDZ")
+    ref = rhf(bs, conv=1e-8, incremental=False)
+    fb = ref["builder"]
+    sch = rhf(bs, fb, conv=1e-8, ifthrs_schedule=True)
+    mix = rhf(bs, fb, conv=1e-8, ifthrs_schedule=True, mixed_cutoff=1e-6)
+    assert abs(sch["energy"] - ref["energy"]) < 1e-8
+    assert abs(mix["energy"] - ref["energy"]) < 1e-7
+    assert min(sch["ifthrs"]) < max(sch["ifthrs"]) <= 20  # the threshold tightened along the way
+
+
 def test_shards_sum_to_full(cuda):
     bs = build_basis(molecules.water_cluster(4, (2, 2, 1), seed=1), "cc-pVDZ")
     fb = FockBuilder(bs)
