@@ -75,3 +75,22 @@ def test_fock_water_cluster_ccpvdz(cuda, orc):
     assert np.abs(f_gpu - f_ref).max() < TOL
     st = fb.last_stats
     assert st["quartets_fp64"] == st["quartets_total"] > 0
+
+
+def test_f_shells_mixed_and_tuned_match_fp64(cuda, orc):
+    """cc-pVTZ (f shells): the single-primitive thread kernels of the f
+    classes, their FP32 half and the warp-team candidates, once autotuned,
+    reproduce the FP64 oracle (FP64 to 1e-10, mixed to 1e-5)."""
+    import torch
+
+    bs = build_basis(methane(), "cc-pVTZ")
+    fb = FockBuilder(bs)
+    d = rand_density(bs.nbf, 12)
+    ref = orc.fock(bs, d, 13, 1.0, 1e-12)
+    dt = torch.tensor(d, device=cuda)
+    fb.autotune(dt, mixed_cutoff=1e-6)
+    f64 = fb.herfck_device(dt).cpu().numpy()
+    assert np.abs(f64 - ref).max() < TOL
+    fmx = fb.herfck_device(dt, mixed_cutoff=1e-6).cpu().numpy()
+    assert np.abs(fmx - ref).max() < 1e-5
+    assert abs(0.5 * float(np.sum(d * (fmx - f64)))) < 1e-6
