@@ -32,6 +32,9 @@ sys.path.insert(0, ROOT)
 METRIC = "J+K build ms & ERI quartets/s, mixed vs FP64 at <=1e-6 Eh; HF gradient ms"
 MIXED_CUTOFF = 1e-6
 THRS = 1e-12
+# dgf_class_time.kernel: thread-per-quartet, cooperative team, warp teams, thread-per-quartet with the density
+# tile, warp-per-quartet
+KERNEL_KIND = ("thread", "team", "team", "thread", "warp")
 
 
 def parse():
@@ -45,6 +48,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gradient", action="store_true")
+    ap.add_argument("--no-extra-configs", action="store_true",
+                    help="skip the (H2O)4, C20H42 and batch legs")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run warmup+steps builds of a core-guess density (for ncu captures)")
     ap.add_argument("--mixed", action="store_true", help="with --profile-run: mixed form")
@@ -144,8 +149,11 @@ def dist_setup(args):
 
 
 def cpu_baseline_sample(bs, dmat, target_s, threads=0):
-    """Oracle (CPU restatement of Dalton's HERMIT J+K) on every stride-th bra
-    pair of the same workload, sized to ~target_s seconds."""
+    """Oracle (CPU restatement of Dalton's HERMIT J+K) timed class by class:
+    every quartet class of the workload is counted, an evenly spaced sample
+    of each class is evaluated and digested on all host cores, and the whole
+    build's time is the sum of count x sampled seconds per quartet
+    (class-stratified, so the class mix is the workload's own)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import orc
 
@@ -154,28 +162,33 @@ def cpu_baseline_sample(bs, dmat, target_s, threads=0):
         orc.set_threads(threads)
     cores = orc.threads()
     t0 = time.perf_counter()
-    orc.fock_sampled(bs, dmat, 1 << 30, 0, THRS)  # set-up only (Schwarz pre-pass)
-    overhead = time.perf_counter() - t0
-    stride = 4000
-    t0 = time.perf_counter()
-    _, nq = orc.fock_sampled(bs, dmat, stride, 0, THRS)
-    dt = max(time.perf_counter() - t0 - overhead, 1e-3)
-    rate = nq / dt
-    total_pairs_frac = 1.0 / stride
-    # second, larger sample sized to the target time
-    want_q = rate * target_s
-    stride2 = max(1, int(nq * stride / max(want_q, 1.0)))
-    if stride2 < stride:
-        t0 = time.perf_counter()
-        _, nq = orc.fock_sampled(bs, dmat, stride2, 0, THRS)
-        dt = max(time.perf_counter() - t0 - overhead, 1e-3)
-        rate = nq / dt
-        total_pairs_frac = 1.0 / stride2
+    r = orc.fock_class_sample(bs, dmat, THRS, target_s)
+    wall = time.perf_counter() - t0
+    rate = r["quartets"] / r["est_seconds"]
+    nsample = sum(c["sample"] for c in r["classes"])
     return {"value": rate, "unit": "quartets/s", "cores": cores, "kind": "port",
-            "sample": f"oracle J+K (CPU restatement of Dalton HERMIT; Dalton itself needs gfortran, absent) on "
-                      f"every {int(round(1 / total_pairs_frac))}-th bra shell pair of the same workload: "
-                      f"{nq} quartets in {dt:.2f} s (Schwarz pre-pass excluded)",
-            "seconds": dt, "quartets": nq}
+            "sample": f"oracle J+K (C++ restatement of Dalton's HERMIT McMurchie-Davidson build and FCKCON "
+                      f"digestion; Dalton itself needs gfortran, absent here) timed class by class: "
+                      f"{len(r['classes'])} quartet classes, {nsample} sampled quartets of {r['quartets']}, "
+                      f"extrapolated full build {r['est_seconds']:.1f} s on {cores} threads; unlike HERMIT it "
+                      f"evaluates general contractions (cc-pVDZ O 1s/2s, H 1s) as separate segmented shells, "
+                      f"so it repeats their primitive integrals",
+            "est_full_build_s": r["est_seconds"], "quartets": r["quartets"], "wall_s": wall}
+
+
+def workload_config(name, bs, mol, basis):
+    """The `config` both arms print for a workload (same dict, same string)."""
+    return {"workload": f"{name}: (H2O)32 cluster (seeded), {basis}, {bs.nbf} spherical basis functions, "
+                        f"J+K IFCTYP 13, Schwarz {THRS}, RHF density after 12 SCF iterations"}
+
+
+def bench_density(bs):
+    """The timed density: RHF after 12 SCF iterations, read from the stored
+    occupied orbitals (tests/golden/make_bench_density.py writes them)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_bench_density
+
+    return make_bench_density.load_density(bs)
 
 
 def run_reference(args):
@@ -187,16 +200,11 @@ def run_reference(args):
 
     mol, basis = molecules.config(args.workload)
     bs = build_basis(mol, basis)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import orc
-
-    orc.build()
-    # A fixed, physically shaped density: the oracle's SCF is too slow at this
-    # size, so use a superposition-of-monomers guess (same quartet set: the
-    # Schwarz screen does not depend on D).
-    rng = np.random.default_rng(0)
-    d = rng.normal(size=(bs.nbf, bs.nbf)) * 1e-3
-    d = d + d.T + np.eye(bs.nbf) * 0.5
+    d = bench_density(bs)
+    if d is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the stored benchmark density "
+                          "(tests/golden/h2o32_ccpvdz_scf12_cocc.npz) is missing"}), flush=True)
+        return
     per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
     vals = []
     info = None
@@ -208,8 +216,9 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "quartets/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {mol.natom} atoms, {basis}, {bs.nbf} basis functions, "
-                                   f"J+K IFCTYP 13, Schwarz {THRS}", "cpu_sample_per_step_s": per_step},
+            "config": workload_config(args.workload, bs, mol, basis),
+            "cpu_sample_per_step_s": per_step,
+            "step_values": vals,
             "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": info["cores"], "kind": "port",
                              "sample": info["sample"]},
             "e2e": {"value": v, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -264,6 +273,10 @@ def best_choices(tuning):
 
 
 def run_batch(args):
+    print(json.dumps(batch_leg(args.workload, args.steps, args.warmup)), flush=True)
+
+
+def batch_leg(workload, steps, warmup):
     """Batched J+K of many molecules: one graph-replayed launch sequence vs a
     per-molecule launch loop (same contexts, same densities)."""
     import torch
@@ -273,7 +286,7 @@ def run_batch(args):
     from dalton_b200.batch import BatchBuilder
     from dalton_b200.fock import FockBuilder
 
-    mols, basis = molecules.config(args.workload)
+    mols, basis = molecules.config(workload)
     dev = torch.device("cuda", 0)
     t0 = time.perf_counter()
     fbs = [FockBuilder(build_basis(m, basis)) for m in mols]
@@ -297,16 +310,16 @@ def run_batch(args):
     stream = torch.cuda.current_stream(dev)
 
     def timed(fn):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             fn()
         e1.record(stream)
         e1.synchronize()
-        return e0.elapsed_time(e1) / args.steps
+        return e0.elapsed_time(e1) / steps
 
     def loop():
         for fb, d, o in zip(fbs, ds, outs):
@@ -320,15 +333,150 @@ def run_batch(args):
     loop()
     torch.cuda.synchronize(dev)
     err = max(float(torch.max(torch.abs(a - b))) for a, b in zip(bb.unpack(fp), outs))
-    line = {"workload": f"{args.workload}: {len(mols)} water clusters of 1-16 molecules (seeded), {basis}, "
+    for fb in fbs:
+        fb.close()
+    return {"workload": f"{workload}: {len(mols)} water clusters of 1-16 molecules (seeded), {basis}, "
                         f"{sum(fb.nbf for fb in fbs)} basis functions in all, J+K IFCTYP 13, Schwarz {THRS}",
-            "quartets": st["quartets_total"], "steps": args.steps, "warmup": args.warmup,
+            "quartets": st["quartets_total"], "steps": steps, "warmup": warmup,
             "per_molecule_loop_ms": loop_ms, "batched_graph_ms": graph_ms, "batched_no_graph_ms": nograph_ms,
             "speedup_graph_vs_loop": loop_ms / graph_ms, "quartets_per_s_graph": st["quartets_total"] / (graph_ms * 1e-3),
             "launches_batched": st["kernel_launches"], "max_abs_diff_vs_loop": err, "context_setup_s": setup_s,
             "autotune_s_largest_molecule": tune_s,
             "data": "synthetic (seeded clusters, guess-like densities)"}
-    print(json.dumps(line), flush=True)
+
+
+def core_guess_density(fb, mol):
+    """Closed-shell density of the core-Hamiltonian orbitals (a guess-like density)."""
+    import torch
+
+    S, T, V = fb.oneint()
+    Hm = torch.tensor(T + V, device="cuda")
+    Sm = torch.tensor(S, device="cuda")
+    s, U = torch.linalg.eigh(Sm)
+    X = U / torch.sqrt(s)
+    _, C = torch.linalg.eigh(X.T @ Hm @ X)
+    C = X @ C
+    nocc = mol.nelectrons() // 2
+    return (2.0 * C[:, :nocc] @ C[:, :nocc].T).contiguous(), torch.tensor(T + V, device="cuda")
+
+
+def timed_builds(fb, D, steps, warmup, flush, mixed_cutoff=0.0):
+    """Mean device ms of one J+K build (CUDA events on the launching stream,
+    L2 flushed before every step)."""
+    import torch
+
+    stream = torch.cuda.current_stream()
+    out = torch.empty_like(D)
+    for _ in range(warmup):
+        fb.herfck_device(D, fmat=out, mixed_cutoff=mixed_cutoff, stats=False)
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fb.herfck_device(D, fmat=out, mixed_cutoff=mixed_cutoff, stats=False)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total / steps, out
+
+
+def top_kernel(fb, D, mixed_cutoff, fp64_peak, fp32_peak):
+    """Per-launch profile of one build: the dominant class kernel with its
+    model FLOP rate and fraction of the measured FMA peak."""
+    from dalton_b200.perfmodel import class_flops
+
+    fb.set_profiling(True)
+    fb.herfck_device(D, mixed_cutoff=mixed_cutoff)
+    prof = fb.profile()
+    fb.set_profiling(False)
+    agg = {}
+    for r in prof:
+        k = (r["la"], r["lb"], r["lc"], r["ld"], r["precision"], r["kernel"])
+        a = agg.setdefault(k, {"ms": 0.0, "evaluated": 0, "prim_quartets": 0})
+        a["ms"] += r["ms"]
+        a["evaluated"] += r["evaluated"]
+        a["prim_quartets"] += r["prim_quartets"]
+    k, a = max(agg.items(), key=lambda kv: kv[1]["ms"])
+    flops = class_flops(k[0], k[1], k[2], k[3], a["prim_quartets"], a["evaluated"])
+    peak = fp64_peak if k[4] == 64 else fp32_peak
+    ach = flops / (a["ms"] * 1e-3) / 1e12
+    tot = sum(v["ms"] for v in agg.values())
+    return {"kernel": f"jk_{KERNEL_KIND[k[5]]}_kernel<{k[0]},{k[1]},{k[2]},{k[3]},"
+                      f"{'double' if k[4] == 64 else 'float'}>", "ms": a["ms"], "quartets": a["evaluated"],
+            "achieved_tflops": ach, "peak_tflops": peak, "frac": ach / peak, "share_of_build": a["ms"] / tot}
+
+
+def small_leg(args, flush, fp64_peak, fp32_peak):
+    """C1: (H2O)4 / cc-pVDZ, FP64 J+K at the converged RHF density and the
+    full SCF energy; the oracle's full build of the same density on the host
+    cores beside it."""
+    from dalton_b200 import molecules
+    from dalton_b200.basis import build_basis
+    from dalton_b200.scf import rhf
+
+    mol, basis = molecules.config("h2o4_ccpvdz")
+    bs = build_basis(mol, basis)
+    res = rhf(bs, conv=1e-9, incremental=False, thrs=THRS)
+    fb = res["builder"]
+    D = res["dmat"].contiguous()
+    ms, _ = timed_builds(fb, D, args.steps, args.warmup, flush)
+    quartets = fb.ao_quartets(THRS)
+    out = {"workload": f"h2o4_ccpvdz: (H2O)4 cluster (seeded), {basis}, {bs.nbf} spherical basis functions, "
+                       f"J+K IFCTYP 13, Schwarz {THRS}, converged RHF density",
+           "fp64_ms": ms, "quartets": quartets, "quartets_per_s": quartets / (ms * 1e-3),
+           "scf_energy": res["energy"], "scf_iterations": res["niter"],
+           "top_kernel": top_kernel(fb, D, 0.0, fp64_peak, fp32_peak)}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import orc
+
+        orc.build()
+        d = D.cpu().numpy()
+        t0 = time.perf_counter()
+        orc.fock(bs, d, 13, 1.0, THRS)
+        out["oracle_full_build_s"] = time.perf_counter() - t0
+        out["oracle_threads"] = orc.threads()
+    fb.close()
+    return out
+
+
+def alkane_leg(args, flush, fp64_peak, fp32_peak):
+    """C3: C20H42 / cc-pVTZ (f shells), per-class autotuned kernels, FP64 and
+    mixed J+K at the core-Hamiltonian guess density."""
+    import torch
+
+    from dalton_b200 import molecules
+    from dalton_b200.basis import build_basis
+    from dalton_b200.fock import FockBuilder
+
+    mol, basis = molecules.config("c20h42_ccpvtz")
+    bs = build_basis(mol, basis)
+    t0 = time.perf_counter()
+    fb = FockBuilder(bs)
+    setup_s = time.perf_counter() - t0
+    D, H = core_guess_density(fb, mol)
+    steps, warmup = max(2, min(args.steps, 3)), 1
+    ms_untuned, _ = timed_builds(fb, D, steps, warmup, flush)
+    t0 = time.perf_counter()
+    fb.autotune(D, thrs=THRS, mixed_cutoff=MIXED_CUTOFF)
+    tune_s = time.perf_counter() - t0
+    ms64, F64 = timed_builds(fb, D, steps, warmup, flush)
+    F64 = F64.clone()
+    msmx, Fmx = timed_builds(fb, D, steps, warmup, flush, MIXED_CUTOFF)
+    dE = abs(0.5 * float(torch.sum(D * (Fmx - F64))))
+    quartets = fb.ao_quartets(THRS)
+    out = {"workload": f"c20h42_ccpvtz: all-trans C20H42 (seeded jitter), {basis}, {bs.nbf} spherical basis "
+                       f"functions (up to f), J+K IFCTYP 13, Schwarz {THRS}, core-Hamiltonian guess density",
+           "fp64_ms_default_kernels": ms_untuned, "autotune_s": tune_s, "context_s": setup_s,
+           "fp64_ms": ms64, "mixed_ms": msmx, "speedup_mixed_vs_fp64": ms64 / msmx,
+           "mixed_energy_error_Eh": dE, "mixed_max_abs_dF": float(torch.max(torch.abs(Fmx - F64))),
+           "quartets": quartets, "quartets_per_s_fp64": quartets / (ms64 * 1e-3),
+           "quartets_per_s_mixed": quartets / (msmx * 1e-3),
+           "top_kernel_fp64": top_kernel(fb, D, 0.0, fp64_peak, fp32_peak)}
+    fb.close()
+    return out
 
 
 def main():
@@ -376,10 +524,20 @@ def main():
             pg.all_reduce(F)
         return F
 
-    # Density of the timed builds: 12-iteration RHF with FP64 builds (replicated on every rank).
-    scf64 = rhf(bs, fb, maxiter=args.scf_iters, fixed_iterations=args.scf_iters, thrs=THRS)
-    D = scf64["dmat"].contiguous()
-    H = scf64["H"]
+    # Density of the timed builds: RHF after 12 SCF iterations with FP64
+    # builds, read from the stored orbitals that the CPU reference arm reads
+    # too (recomputed when they are missing).
+    D_np = bench_density(bs) if args.scf_iters == 12 else None
+    density_source = "stored (tests/golden/h2o32_ccpvdz_scf12_cocc.npz)"
+    if D_np is None:
+        scf64 = rhf(bs, fb, maxiter=args.scf_iters, fixed_iterations=args.scf_iters, thrs=THRS)
+        D = scf64["dmat"].contiguous()
+        density_source = f"computed ({args.scf_iters} SCF iterations in this run)"
+    else:
+        D = torch.tensor(D_np, device=dev)
+    S_np, T_np, V_np = fb.oneint()
+    H = torch.tensor(T_np + V_np, device=dev)
+    enuc = mol.nuclear_repulsion()
     # Per-class kernel choice on this density (FP64 and FP32 candidates, mixed split).
     t0 = time.perf_counter()
     tuning = fb.autotune(D, thrs=THRS, mixed_cutoff=MIXED_CUTOFF)
@@ -393,7 +551,6 @@ def main():
         scf_inc = rhf(bs, fb, conv=1e-6, maxiter=60, thrs=THRS, ifthrs_schedule=True)
         scf_mix = rhf(bs, fb, conv=1e-6, maxiter=60, thrs=THRS, mixed_cutoff=MIXED_CUTOFF, ifthrs_schedule=True)
     scf_s = time.perf_counter() - t0
-    enuc = scf64["enuc"]
     # Accuracy of the mixed build at the converged density.
     F64 = build(D, False).clone()
     Fmx = build(D, True).clone()
@@ -490,14 +647,13 @@ def main():
     achieved = top_flops / (top["ms"] * 1e-3) / 1e12
     peak = fp64_peak if top["precision"] == 64 else fp32_peak
     tot_ms = sum(r["ms"] for r in prof)
+    kname = lambda r: (f"jk_{KERNEL_KIND[r['kernel']]}_kernel<{r['la']},{r['lb']},{r['lc']},{r['ld']},"
+                       f"{'double' if r['precision'] == 64 else 'float'}>")
     roofline = {"bound": "fp64" if top["precision"] == 64 else "fp32",
-                "kernel": f"jk_{('thread', 'team', 'team')[top['kernel']]}_kernel<{top['la']},{top['lb']},"
-                          f"{top['lc']},{top['ld']},{'double' if top['precision'] == 64 else 'float'}>",
+                "kernel": kname(top),
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": "measured FMA-loop peak on this GPU (MEASURED_PEAKS.json has no FP64 figure)",
-                "traffic": ncu_traffic(f"jk_{('thread', 'team', 'team')[top['kernel']]}_kernel<{top['la']},{top['lb']},"
-                                       f"{top['lc']},{top['ld']},{'double' if top['precision'] == 64 else 'float'}>",
-                                       args.workload),
+                "traffic": ncu_traffic(kname(top), args.workload),
                 "share_of_build": top["ms"] / tot_ms if tot_ms else None,
                 "flops_model": "dalton_b200/perfmodel.py (per primitive and per contracted quartet)"}
     all_flops = sum(class_flops(r["la"], r["lb"], r["lc"], r["ld"], r["prim_quartets"], r["evaluated"]) for r in prof)
@@ -535,6 +691,12 @@ def main():
                      "translational_sum": float(np.abs(gfull.sum(0)).max())}
         gfb.close()
 
+    legs = {}
+    if world == 1 and not args.no_extra_configs:
+        legs["c1"] = small_leg(args, flush, fp64_peak, fp32_peak)
+        legs["c3"] = alkane_leg(args, flush, fp64_peak, fp32_peak)
+        legs["c4"] = batch_leg("batch256_631gs", max(2, min(args.steps, 3)), 2)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(bs, D.cpu().numpy(), args.cpu_seconds)
@@ -546,11 +708,9 @@ def main():
             "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64+f32 (mixed)" if headline_mixed else "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: (H2O)32 cluster (seeded), {basis}, {bs.nbf} spherical basis "
-                                   f"functions, J+K IFCTYP 13, Schwarz {THRS}, RHF density after "
-                                   f"{args.scf_iters} SCF iterations",
-                       "mixed_cutoff": MIXED_CUTOFF, "parallelism": f"quartet-queue shards x{world}",
-                       "l2": "flushed (256 MB write) before every timed step"},
+            "config": workload_config(args.workload, bs, mol, basis),
+            "run": {"mixed_cutoff": MIXED_CUTOFF, "parallelism": f"cost-weighted quartet-queue shards x{world}",
+                    "l2": "flushed (256 MB write) before every timed step", "density": density_source},
             "fp64": {"ms": ms64, "quartets_per_s": quartets / (ms64 * 1e-3), "quartets": quartets,
                      "working_basis_quartets": q64},
             "mixed": {"ms": msmx, "quartets_per_s": quartets / (msmx * 1e-3), "quartets": quartets,
@@ -564,6 +724,7 @@ def main():
             "peaks_measured": {"fp64_tflops": fp64_peak, "fp32_tflops": fp32_peak},
             "gpu_launches": int((lmx if headline_mixed else l64)),
             "hf_gradient": grad_info,
+            "c1": legs.get("c1"), "c3": legs.get("c3"), "c4": legs.get("c4"),
             "clocks": clk, "cpu_baseline": cpu,
             "profile_top": [{k: r[k] for k in ("la", "lb", "lc", "ld", "precision", "kernel", "evaluated",
                                                "prim_quartets", "ms")} for r in by_time[:8]],

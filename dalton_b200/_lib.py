@@ -34,7 +34,8 @@ class DgfBasis(ctypes.Structure):
 
 class DgfOptions(ctypes.Structure):
     _fields_ = [("thrs", ctypes.c_double), ("ifthrs", dgf_int), ("hfxfac", ctypes.c_double),
-                ("mixed_cutoff", ctypes.c_double), ("shard_index", dgf_int), ("shard_count", dgf_int)]
+                ("mixed_cutoff", ctypes.c_double), ("shard_index", dgf_int), ("shard_count", dgf_int),
+                ("icedif", dgf_int)]
 
 
 class DgfStats(ctypes.Structure):

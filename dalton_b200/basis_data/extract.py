@@ -45,4 +45,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/basis")
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract.py <path to the basis/ folder of a Dalton source tree>")
+    main(sys.argv[1])

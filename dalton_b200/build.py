@@ -78,16 +78,29 @@ def _generated_units():
     gen = os.path.join(BUILD, "gen")
     os.makedirs(gen, exist_ok=True)
     units = []
-    for kind, header, macro, n in (("jk", "dgf_jk_inst.cuh", "DGF_JK_CLASS", NUM_PAIR_CLASS),
-                                   ("grad", "dgf_grad_kernel.cuh", "DGF_GRAD_CLASS", NUM_GRAD_CLASS)):
+    for kind, header, macro, n, parts in (("jk", "dgf_jk_inst.cuh", "DGF_JK_CLASS", NUM_PAIR_CLASS, 3),
+                                          ("grad", "dgf_grad_kernel.cuh", "DGF_GRAD_CLASS", NUM_GRAD_CLASS, 0)):
         for x in range(n):
             for y in range(x + 1):
-                path = os.path.join(gen, f"dgf_{kind}_{x}_{y}.cu")
-                text = f'#include "{header}"\n\n{macro}({x}, {y})\n'
-                if not os.path.exists(path) or open(path).read() != text:
-                    with open(path, "w") as f:
-                        f.write(text)
-                units.append((_class_l(x) + _class_l(y), path))
+                for part in (range(parts) if parts else [None]):
+                    if part is None:
+                        path = os.path.join(gen, f"dgf_{kind}_{x}_{y}.cu")
+                        text = f'#include "{header}"\n\n{macro}({x}, {y})\n'
+                    else:
+                        path = os.path.join(gen, f"dgf_{kind}_{x}_{y}_{part}.cu")
+                        text = f'#include "{header}"\n\n{macro}({x}, {y}, {part})\n'
+                    if not os.path.exists(path) or open(path).read() != text:
+                        with open(path, "w") as f:
+                            f.write(text)
+                    units.append((_class_l(x) + _class_l(y), path))
+    # drop objects of units that are no longer generated (an earlier layout)
+    keep = {os.path.basename(p).replace(".cu", ".o") for _, p in units}
+    for o in glob.glob(os.path.join(BUILD, "dgf_jk_*.o")):
+        if os.path.basename(o) not in keep:
+            os.remove(o)
+    for g in glob.glob(os.path.join(gen, "dgf_jk_*.cu")):
+        if os.path.basename(g).replace(".cu", ".o") not in keep:
+            os.remove(g)
     return [p for _, p in sorted(units, key=lambda u: -u[0])]
 
 

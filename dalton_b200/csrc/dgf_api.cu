@@ -182,7 +182,7 @@ static void free_ctx(dgf_ctx *c) {
   cudaSetDevice(c->device);
   void *ptrs[] = {c->d_pairs, c->d_pp,     c->d_boys,   c->d_sph,   c->d_D,     c->d_Ds,    c->d_Fh, c->d_io,
                   c->d_dmax,  c->d_cnt,    c->d_qoff,   c->d_wmap_i, c->d_wmap_c, c->d_wmeta, c->d_wdims, c->d_gw,
-                  c->d_shinfo};
+                  c->d_shinfo, c->d_blk_gab, c->d_blk_info, c->d_blk_dmax};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -202,9 +202,10 @@ static const ClassKernel &select_kernel(const dgf_ctx *c, int X, int Y, int prec
   if (precision == 2) return jk_kernel(X, Y, 2);
   const int p = precision ? 1 : 0;
   const int v = c->choice[X][Y][p];
-  const ClassKernel &k = jk_kernel_variant(X, Y, p, v, ket1);
+  const bool bra1 = c->cls_max_npp[X] == 1;
+  const ClassKernel &k = jk_kernel_variant(X, Y, p, v, ket1, bra1);
   if (k.launch) return k;
-  return jk_kernel(X, Y, precision, ket1);
+  return jk_kernel(X, Y, precision, ket1, bra1);
 }
 
 static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs &args, cudaStream_t st,
@@ -218,12 +219,31 @@ static int launch_class(dgf_ctx *c, int X, int Y, JKArgs &args, cudaStream_t st,
 static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs &args, cudaStream_t st,
                          int precision) {
   if (!k.launch) DGF_FAIL(DGF_ERR_UNSUPPORTED, "no kernel for this class and precision");
-  const bool thread_kernel = (k.smem == 0);
+  const bool thread_kernel = (k.kind == kKindThread);
   const int64_t per_block = k.qpb;  // thread kernels: a quartet per thread; team kernels: per block or per warp
   const int64_t nq = args.nquartet - args.q_begin;
   if (nq <= 0 && !args.diag_out) return DGF_OK;
-  int64_t grid64 = std::min<int64_t>((nq + per_block - 1) / per_block, (int64_t)c->nsm * 16);
+  int64_t grid64 = std::min<int64_t>((nq + per_block - 1) / per_block, (int64_t)c->nsm * (thread_kernel ? 8 : 16));
   int grid = (int)std::max<int64_t>(grid64, 1);
+  // Tiled digestion: one density slot, bra rows that fit in shared memory,
+  // and long enough runs of kets per bra for the tile flushes to pay.
+  size_t smem = k.smem;
+  args.tile_rows = args.tile_fa = args.tile_n = 0;
+  if (thread_kernel && c->tile_enabled && args.nslot == 1 && !args.kbase && !args.diag_out && k.occ) {
+    const int la = cls_l1(X), lb = X - la * (la + 1) / 2;
+    const int fa = nfun(la, c->spherical), fb = nfun(lb, c->spherical);
+    const size_t bytes = (size_t)(fa + fb) * c->nwf * sizeof(double);
+    if (bytes <= kTileMaxBytes && nq >= kTileMinQuartetsPerBra * (int64_t)args.nbra) {
+      const int occ = k.occ(bytes);
+      if (occ > 0) {
+        args.tile_rows = fa + fb;
+        args.tile_fa = fa;
+        args.tile_n = c->nwf;
+        smem = bytes;
+        grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->nsm * occ, (nq + 255) / 256));
+      }
+    }
+  }
   const bool prof = c->profiling && !args.diag_out;
   if (prof) {
     cudaEvent_t e0, e1;
@@ -233,7 +253,7 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
     c->prof_ev.push_back(e1);
     DGF_CUDA_CHECK(cudaEventRecord(e0, st));
   }
-  k.launch(args, grid, k.block, k.smem, st);
+  k.launch(args, grid, k.block, smem, st);
   DGF_CUDA_CHECK(cudaGetLastError());
   if (prof) {
     DGF_CUDA_CHECK(cudaEventRecord(c->prof_ev.back(), st));
@@ -243,7 +263,7 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
     r.lc = cls_l1(Y);
     r.ld = Y - r.lc * (r.lc + 1) / 2;
     r.precision = (precision == 1) ? 32 : 64;
-    r.kernel = thread_kernel ? 0 : (k.qpb > 1 ? 2 : 1);
+    r.kernel = thread_kernel ? (args.tile_rows ? 3 : 0) : k.kind == kKindWarpTeam ? 2 : k.kind == kKindWarp ? 4 : 1;
     (void)k;
     r.quartets = args.nquartet - args.q_begin;
     r.evaluated = 0;
@@ -398,6 +418,7 @@ static int compute_schwarz(dgf_ctx *c) {
 struct ShellList {
   const std::vector<int> &l, &atom, &ao, &nprim, &p0;
   const std::vector<double> &a, &c;
+  const std::vector<int> *blk = nullptr;  // Dalton block of each shell (PairRec blkA/blkB), with kWholeBlock
 };
 
 // Shell pairs A >= B (the higher l first) with their primitive pairs, class
@@ -426,6 +447,8 @@ static void build_pairs(const dgf_ctx *c, const ShellList &sh, int nbfm, std::ve
       r.same = (A == B);
       r.atA = sh.atom[sa];
       r.atB = sh.atom[sb];
+      r.blkA = sh.blk ? (*sh.blk)[sa] : 0;
+      r.blkB = sh.blk ? (*sh.blk)[sb] : 0;
       r.nbfm = nbfm;
       r.dbase = 0;
       r.pp0 = (int)pp.size();
@@ -494,6 +517,7 @@ static int build_working_basis(dgf_ctx *c, const dgf_basis *b) {
         c->ws_atom.push_back(at);
         c->ws_ao.push_back(wao);
         c->ws_p0.push_back((int)c->ws_a.size());
+        c->ws_blk.push_back((int)ib);
         c->ws_nprim.push_back(1);
         c->ws_a.push_back(ex[i]);
         c->ws_c.push_back(scale);
@@ -513,6 +537,7 @@ static int build_working_basis(dgf_ctx *c, const dgf_basis *b) {
         c->ws_atom.push_back(at);
         c->ws_ao.push_back(wao);
         c->ws_p0.push_back((int)c->ws_a.size());
+        c->ws_blk.push_back((int)ib);
         int cnt = 0;
         for (int i = 0; i < np; ++i) {
           const double v = cf[(size_t)k * np + i];
@@ -600,6 +625,7 @@ extern "C" void dgf_default_options(dgf_options *opt) {
   opt->mixed_cutoff = 0.0;
   opt->shard_index = 0;
   opt->shard_count = 1;
+  opt->icedif = 3;
 }
 
 extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
@@ -618,6 +644,10 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
   if (device < 0 || device >= ndev) DGF_FAIL(DGF_ERR_ARG, "device index out of range");
   std::unique_ptr<dgf_ctx, void (*)(dgf_ctx *)> c(new dgf_ctx, free_ctx);
   c->device = device;
+  {
+    const char *nt = getenv("DGF_NO_TILE");
+    c->tile_enabled = !(nt && nt[0] == '1');
+  }
   DeviceGuard g(device);
   cudaDeviceProp prop;
   DGF_CUDA_CHECK(cudaGetDeviceProperties(&prop, device));
@@ -644,6 +674,7 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
       c->sh_atom.push_back(at);
       c->sh_ao.push_back(ao);
       c->sh_p0.push_back((int)c->sh_a.size());
+      c->sh_blk.push_back((int)ib);
       int cnt = 0;
       for (int i = 0; i < np; ++i) {
         const double cc = b->coef[b->block_coef_offset[ib] + (dgf_int)k * np + i];
@@ -664,9 +695,26 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
   int st_wb = build_working_basis(c.get(), b);
   if (st_wb) return st_wb;
 
+  // Dalton blocks: working shells per block (a block that is one working
+  // shell is "whole"), and each block's AO functions.
+  c->nblk = (int)b->nblock;
+  {
+    std::vector<int> nws(c->nblk, 0);
+    for (int blk : c->ws_blk) ++nws[blk];
+    c->ws_blk_flag.resize(c->ws_blk.size());
+    for (size_t i = 0; i < c->ws_blk.size(); ++i)
+      c->ws_blk_flag[i] = c->ws_blk[i] | (nws[c->ws_blk[i]] == 1 ? kWholeBlock : 0);
+    c->blk_ao0.resize(c->nblk);
+    c->blk_nf.resize(c->nblk);
+    for (int ib = 0; ib < c->nblk; ++ib) {
+      c->blk_ao0[ib] = (int)b->block_ao_offset[ib];
+      c->blk_nf[ib] = (int)b->block_ncontr[ib] * nfun((int)b->block_l[ib], c->spherical);
+    }
+  }
   // Working-basis shell pairs with their primitive pairs.
-  build_pairs(c.get(), ShellList{c->ws_l, c->ws_atom, c->ws_ao, c->ws_nprim, c->ws_p0, c->ws_a, c->ws_c}, c->nwf,
-              c->pairs, c->cls_off, c->pp);
+  build_pairs(c.get(),
+              ShellList{c->ws_l, c->ws_atom, c->ws_ao, c->ws_nprim, c->ws_p0, c->ws_a, c->ws_c, &c->ws_blk_flag},
+              c->nwf, c->pairs, c->cls_off, c->pp);
 
   DGF_CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   DGF_CUDA_CHECK(cudaEventCreate(&c->ev0));
@@ -707,6 +755,13 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
       while (b < kNumBuckets && pos < n && npp_bucket(c->pairs[c->cls_off[X] + pos].npp) < b) ++pos;
       c->bkt_off[X][b] = (b == kNumBuckets) ? n : pos;
     }
+  }
+  for (int X = 0; X < kNumPairClass; ++X) {
+    double sum = 0.0;
+    for (int i = c->cls_off[X]; i < c->cls_off[X + 1]; ++i) sum += c->pairs[i].npp;
+    c->cls_avg_npp[X] = c->cls_off[X + 1] > c->cls_off[X] ? sum / (c->cls_off[X + 1] - c->cls_off[X]) : 0.0;
+    c->cls_max_npp[X] = 0;
+    for (int i = c->cls_off[X]; i < c->cls_off[X + 1]; ++i) c->cls_max_npp[X] = std::max(c->cls_max_npp[X], c->pairs[i].npp);
   }
   // Primitive pairs in the order of the sorted pair list.
   {
@@ -884,7 +939,9 @@ static int ensure_slots(dgf_ctx *c, int nslot) {
   return DGF_OK;
 }
 
-// Block maxima of |D| per shell pair over all slots (MKDRAO, her2gab.F:1213).
+// Block maxima of |D| per working shell pair over all slots, for the mixed
+// form's precision bound; stored in FP32 rounded up, so that a bound never
+// shrinks below the FP64 value it stands for.
 __global__ void dmax_kernel(const double *__restrict__ D, int nslot, int n, const int *__restrict__ sh_ao,
                             const int *__restrict__ sh_nf, int ns, float *__restrict__ dm) {
   const int64_t tot = (int64_t)ns * ns;
@@ -899,14 +956,156 @@ __global__ void dmax_kernel(const double *__restrict__ D, int nslot, int n, cons
           m = fmax(m, fmax(fabs(Dk[(size_t)p * n + q]), fabs(Dk[(size_t)q * n + p])));
         }
     }
-    dm[e] = (float)m;
+    dm[e] = __double2float_ru(m);
   }
+}
+
+struct SlotSources {
+  int src[kMaxSlots];
+  int nslot;
+};
+
+// Dalton's block density maxima DMRAO (MKDRAO, DALTON/abacus/her2gab.F:1213)
+// of the AO densities: for every pair of Dalton blocks, max |D_pq| over the
+// functions of the two blocks in both orientations, per density slot (the
+// slot's source matrix) into dm_slot[s] and over the chunk's slots into dm.
+// FP32 rounded up.
+__global__ void blk_dmax_kernel(const double *__restrict__ Dao, int n, const int *__restrict__ blk_ao0,
+                                const int *__restrict__ blk_nf, int nb, SlotSources ss, float *__restrict__ dm,
+                                float *__restrict__ dm_slot) {
+  const int64_t tot = (int64_t)nb * nb;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int A = (int)(e / nb), B = (int)(e - (int64_t)A * nb);
+    double m = 0.0;
+    for (int s = 0; s < ss.nslot; ++s) {
+      const double *Dk = Dao + (size_t)ss.src[s] * n * n;
+      double ms = 0.0;
+      for (int i = 0; i < blk_nf[A]; ++i)
+        for (int j = 0; j < blk_nf[B]; ++j) {
+          const int p = blk_ao0[A] + i, q = blk_ao0[B] + j;
+          ms = fmax(ms, fmax(fabs(Dk[(size_t)p * n + q]), fabs(Dk[(size_t)q * n + p])));
+        }
+      dm_slot[(size_t)s * tot + e] = __double2float_ru(ms);
+      m = fmax(m, ms);
+    }
+    dm[e] = __double2float_ru(m);
+  }
+}
+
+// Block Schwarz factors GAB (GABGEN, DALTON/abacus/her2gab.F:1776) for the
+// density screen, once per context: sqrt(max |(ab|ab)|) over the contracted
+// functions of each pair of Dalton blocks, from the Schwarz factors of the
+// AO basis's segmented shells; and the device buffers of the block bounds.
+static int schwarz_of(dgf_ctx *c, const PairRec *d_pairs, const PrimPair *d_pp, const int *cls_off,
+                      std::vector<double> &q);
+
+static int ensure_block_screen(dgf_ctx *c, int nslot) {
+  const size_t nb2 = (size_t)c->nblk * c->nblk;
+  if (!c->d_blk_gab) {
+    std::vector<PairRec> pairs;
+    std::vector<PrimPair> pp;
+    int cls_off[kNumPairClass + 1];
+    build_pairs(c, ShellList{c->sh_l, c->sh_atom, c->sh_ao, c->sh_nprim, c->sh_p0, c->sh_a, c->sh_c, &c->sh_blk},
+                c->nbf, pairs, cls_off, pp);
+    PairRec *d_pairs = nullptr;
+    PrimPair *d_pp = nullptr;
+    if (dev_alloc(&d_pairs, std::max<size_t>(pairs.size(), 1)) != cudaSuccess ||
+        dev_alloc(&d_pp, std::max<size_t>(pp.size(), 1)) != cudaSuccess) {
+      cudaGetLastError();
+      if (d_pairs) cudaFree(d_pairs);
+      DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the AO pair list failed");
+    }
+    cudaError_t e = cudaMemcpy(d_pairs, pairs.data(), pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_pp, pp.data(), pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice);
+    std::vector<double> q;
+    int st = (e == cudaSuccess) ? schwarz_of(c, d_pairs, d_pp, cls_off, q) : DGF_ERR_CUDA;
+    cudaFree(d_pairs);
+    cudaFree(d_pp);
+    if (e != cudaSuccess) DGF_FAIL(DGF_ERR_CUDA, cudaGetErrorString(e));
+    if (st) return st;
+    std::vector<double> gab(nb2, 0.0);
+    for (size_t i = 0; i < pairs.size(); ++i) {
+      const int A = pairs[i].blkA, B = pairs[i].blkB;
+      gab[(size_t)A * c->nblk + B] = std::max(gab[(size_t)A * c->nblk + B], q[i]);
+      gab[(size_t)B * c->nblk + A] = gab[(size_t)A * c->nblk + B];
+    }
+    std::vector<int> info(c->blk_ao0);
+    info.insert(info.end(), c->blk_nf.begin(), c->blk_nf.end());
+    if (dev_alloc(&c->d_blk_gab, nb2) != cudaSuccess || dev_alloc(&c->d_blk_info, info.size()) != cudaSuccess) {
+      cudaGetLastError();
+      DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the block Schwarz factors failed");
+    }
+    DGF_CUDA_CHECK(cudaMemcpy(c->d_blk_gab, gab.data(), nb2 * 8, cudaMemcpyHostToDevice));
+    DGF_CUDA_CHECK(cudaMemcpy(c->d_blk_info, info.data(), info.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  if (nslot > c->cap_blk_slots) {
+    if (c->d_blk_dmax) cudaFree(c->d_blk_dmax);
+    c->d_blk_dmax = nullptr;
+    c->cap_blk_slots = 0;
+    if (dev_alloc(&c->d_blk_dmax, (size_t)(nslot + 1) * nb2) != cudaSuccess) {
+      cudaGetLastError();
+      DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the block density bounds failed");
+    }
+    c->cap_blk_slots = nslot;
+  }
+  return DGF_OK;
 }
 
 struct SlotSpec {
   int src, op;
   double js, ks;
 };
+
+// Model cost of one quartet of a plan entry: the fixed FLOP model of the
+// McMurchie-Davidson kernels (Boys + prefactor, R_tuv, ket and bra
+// contractions per primitive quartet; spherical transform and six-block
+// digestion per contracted quartet), times the primitive quartets of the
+// entry's bucket.  Deterministic, so that every rank cuts the same shards.
+static double entry_cost_per_quartet(const dgf_ctx *c, const ClassPlan &cp) {
+  const int la = cls_l1(cp.X), lb = cp.X - la * (la + 1) / 2, lc = cls_l1(cp.Y), ld = cp.Y - lc * (lc + 1) / 2;
+  const int L = la + lb + lc + ld, lab = la + lb, lcd = lc + ld;
+  double rt = 0.0;
+  for (int j = 1; j <= L; ++j) rt += 3.0 * n3(j);
+  const double prim = 40.0 + 3.0 * L + rt + 2.0 * n3(lab) * n3(lcd) * ncart(lc) * ncart(ld) +
+                      2.0 * n3(lab) * ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+  const double nint = (double)nfun(la, c->spherical) * nfun(lb, c->spherical) * nfun(lc, c->spherical) *
+                      nfun(ld, c->spherical);
+  static const double kBucketPrims[kNumBuckets] = {1, 2, 4, 8, 16, 32, 64};
+  const double bra_prims = c->cls_avg_npp[cp.X] > 0 ? c->cls_avg_npp[cp.X] : 1.0;
+  return prim * bra_prims * kBucketPrims[cp.bucket] + 12.0 * nint;
+}
+
+// Quartet range [q0, q1) of plan entry `e` that shard `r` of `n` evaluates:
+// the plan entries in order form one queue whose cost (entry_cost_per_quartet
+// x quartets) is cut into n equal parts, as Dalton's parallel Fock build
+// distributes cost-sorted shell-pair tasks over its workers
+// (DALTON/abacus/herpar.F:457,1165).  Consecutive shards share their cut
+// points, so the ranges of all shards tile every entry exactly.
+static void shard_range(const dgf_ctx *c, size_t e, int64_t r, int64_t n, int64_t *q0, int64_t *q1) {
+  const ClassPlan &cp = c->plan[e];
+  if (n <= 1) {
+    *q0 = 0;
+    *q1 = cp.nquartet;
+    return;
+  }
+  double total = 0.0, before = 0.0;
+  for (size_t i = 0; i < c->plan.size(); ++i) {
+    const double w = (double)c->plan[i].nquartet * entry_cost_per_quartet(c, c->plan[i]);
+    if (i < e) before += w;
+    total += w;
+  }
+  const double w = (double)cp.nquartet * entry_cost_per_quartet(c, cp);
+  auto cut = [&](int64_t k) -> int64_t {
+    if (k <= 0) return 0;
+    if (k >= n) return cp.nquartet;
+    const double x = total * (double)k / (double)n;
+    if (x <= before) return 0;
+    if (x >= before + w) return cp.nquartet;
+    return std::min<int64_t>(cp.nquartet, (int64_t)std::floor((x - before) / w * (double)cp.nquartet));
+  };
+  *q0 = cut(r);
+  *q1 = cut(r + 1);
+}
 
 static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double *dmat_dev, double *fmat_dev,
                      const dgf_options *opt, cudaStream_t st, dgf_stats *stats) {
@@ -956,10 +1155,21 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   }
   int st_code = build_plan(c, o.thrs);
   if (st_code) return st_code;
+  // Density screening as Dalton's direct Fock build: on when IFTHRS < 16,
+  // IFTHRS < 4 taken as 14 (DALTON/abacus/her2drv.F:520-540).
+  int64_t ifthrs = o.ifthrs;
+  if (ifthrs < 4) ifthrs = 14;
+  const bool doscrn = ifthrs < 16;
+  const bool ice = doscrn && (o.icedif & 3) != 0;
+  const bool need_dmax = o.mixed_cutoff > 0.0;
   const int nslot_total = (int)slots.size();
   const int chunk = std::min(kMaxSlots, std::max(nslot_total, 1));
   st_code = ensure_slots(c, chunk);
   if (st_code) return st_code;
+  if (doscrn) {
+    st_code = ensure_block_screen(c, chunk);
+    if (st_code) return st_code;
+  }
   if (c->profiling) {
     for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
     c->prof_ev.clear();
@@ -967,10 +1177,12 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
   }
   DGF_CUDA_CHECK(cudaMemsetAsync(c->d_cnt, 0, 4 * kCounterSlots * sizeof(unsigned long long), st));
   DGF_CUDA_CHECK(cudaEventRecord(c->ev0, st));
-  const bool need_dmax = (o.ifthrs < 20) || (o.mixed_cutoff > 0.0);
   int64_t launches = 0, total_q = 0, nlaunch_class = 0;
-  for (const ClassPlan &cp : c->plan)
-    total_q += cp.nquartet * (o.shard_index + 1) / o.shard_count - cp.nquartet * o.shard_index / o.shard_count;
+  std::vector<int64_t> sq0(c->plan.size()), sq1(c->plan.size());
+  for (size_t e = 0; e < c->plan.size(); ++e) {
+    shard_range(c, e, o.shard_index, o.shard_count, &sq0[e], &sq1[e]);
+    total_q += sq1[e] - sq0[e];
+  }
   // Zero outputs that have no contributions.
   for (int k = 0; k < ndmat; ++k)
     if (outs[k].zero) DGF_CUDA_CHECK(cudaMemsetAsync(fmat_dev + (size_t)k * n2ao, 0, n2ao * 8, st));
@@ -990,6 +1202,15 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
           c->d_D, ns, N, d_shinfo, d_shinfo + nws, nws, c->d_dmax);
       ++launches;
     }
+    const int64_t nb2 = (int64_t)c->nblk * c->nblk;
+    if (doscrn) {
+      SlotSources ss;
+      ss.nslot = ns;
+      for (int s = 0; s < ns; ++s) ss.src[s] = slots[s0 + s].src;
+      blk_dmax_kernel<<<(int)std::max<int64_t>(1, std::min<int64_t>(nb2 / 128 + 1, c->nsm * 8)), 128, 0, st>>>(
+          dmat_dev, c->nbf, c->d_blk_info, c->d_blk_info + c->nblk, c->nblk, ss, c->d_blk_dmax, c->d_blk_dmax + nb2);
+      ++launches;
+    }
     JKArgs a = base_args(c);
     a.nslot = ns;
     a.D = c->d_D;
@@ -1000,11 +1221,20 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
       a.kscale[s] = slots[s0 + s].ks;
     }
     a.dmax = need_dmax ? c->d_dmax : nullptr;
-    a.dens_thr = (o.ifthrs < 20) ? std::pow(10.0, -(double)o.ifthrs) : 0.0;
+    a.dens_thr = doscrn ? std::pow(10.0, -(double)ifthrs) : 0.0;
+    a.blk_gab = doscrn ? c->d_blk_gab : nullptr;
+    a.blk_dmax = doscrn ? c->d_blk_dmax : nullptr;
+    a.blk_dmax_slot = doscrn ? c->d_blk_dmax + nb2 : nullptr;
+    a.blk_stride = nb2;
+    a.nblk = c->nblk;
+    a.ice_thr = ice ? a.dens_thr : 0.0;
+    a.icedif = (int)(o.icedif & 3);
     a.split = o.mixed_cutoff;
     a.schwarz_thr = o.thrs;
     a.mode = 0;
-    for (const ClassPlan &cp : c->plan) {
+    for (size_t e = 0; e < c->plan.size(); ++e) {
+      const ClassPlan &cp = c->plan[e];
+      if (sq1[e] <= sq0[e]) continue;  // not in this shard
       a.bra = c->d_pairs + c->cls_off[cp.X];
       a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
       a.ket_off = cp.kb0;
@@ -1012,8 +1242,8 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
       a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
       a.same_class = (cp.X == cp.Y);
       a.qoff = c->d_qoff + cp.off;
-      a.q_begin = cp.nquartet * o.shard_index / o.shard_count;
-      a.nquartet = cp.nquartet * (o.shard_index + 1) / o.shard_count;
+      a.q_begin = sq0[e];
+      a.nquartet = sq1[e];
       // Boys table of order L = la+lb+lc+ld.
       const int la = (cp.X == 0) ? 0 : (cp.X <= 2) ? 1 : (cp.X <= 5) ? 2 : 3;
       const int lb = cp.X - la * (la + 1) / 2;
@@ -1021,7 +1251,7 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
       const int ld = cp.Y - lc * (lc + 1) / 2;
       a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
       const bool split = o.mixed_cutoff > 0.0 && c->split_ok[cp.X][cp.Y] &&
-                         jk_kernel(cp.X, cp.Y, 1, cp.bucket == 0).launch != nullptr;
+                         select_kernel(c, cp.X, cp.Y, 1, cp.bucket == 0).launch != nullptr;
       const int Lq = la + lb + lc + ld;
       for (int part = 0; part < (split ? 2 : 1); ++part) {
         a.mode = split ? 1 + part : 0;
@@ -1188,8 +1418,10 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
       float best = 1e30f;
       int bestv = c->choice[cp.X][cp.Y][p];
       a.boys = c->d_boys + (p ? boys_low_offset(la + lb + lc + ld) : (size_t)(la + lb + lc + ld) * kBoysTableDoubles);
-      for (int v = -2; v < kThreadVariants; ++v) {
-        if (!jk_kernel_variant(cp.X, cp.Y, p, v).launch && !jk_kernel_variant(cp.X, cp.Y, p, v, true).launch)
+      const bool bra1 = c->cls_max_npp[cp.X] == 1;
+      for (int v = -3; v < kThreadVariants; ++v) {
+        if (!jk_kernel_variant(cp.X, cp.Y, p, v, false, bra1).launch &&
+            !jk_kernel_variant(cp.X, cp.Y, p, v, true, bra1).launch)
           continue;
         int chunks = 1;
         float ms = 0.f;
@@ -1203,8 +1435,8 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
             a.qoff = c->d_qoff + cq.off;
             a.nquartet = cq.nquartet;
             // entries this candidate has no kernel for run the FP64 default (same for every candidate)
-            const ClassKernel &kv = jk_kernel_variant(cq.X, cq.Y, p, v, cq.bucket == 0);
-            const ClassKernel &k = kv.launch ? kv : jk_kernel(cq.X, cq.Y, 0, cq.bucket == 0);
+            const ClassKernel &kv = jk_kernel_variant(cq.X, cq.Y, p, v, cq.bucket == 0, bra1);
+            const ClassKernel &k = kv.launch ? kv : jk_kernel(cq.X, cq.Y, 0, cq.bucket == 0, bra1);
             if (kv.launch) chunks = k.chunks;
             r = launch_kernel(c, k, cq.X, cq.Y, a, st, kv.launch ? p : 0);
             if (r) return r;
@@ -1226,7 +1458,8 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
     }
     // Mixed form: split the class into FP64 and FP32 launches only where
     // that beats one FP64 pass (both walk all of the class's quartets).
-    if (o.mixed_cutoff > 0.0 && (jk_kernel(cp.X, cp.Y, 1).launch || jk_kernel(cp.X, cp.Y, 1, true).launch)) {
+    if (o.mixed_cutoff > 0.0 &&
+        (select_kernel(c, cp.X, cp.Y, 1, false).launch || select_kernel(c, cp.X, cp.Y, 1, true).launch)) {
       const int Lq = la + lb + lc + ld;
       float t[2] = {0.f, 0.f};
       for (int cfg = 0; cfg < 2; ++cfg) {  // 0: FP64 only, 1: FP64 + FP32 halves
@@ -1242,7 +1475,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
             a.dmax = c->d_dmax;
             a.split = o.mixed_cutoff;
             // as in the build: entries without an FP32 kernel are not split
-            const bool cansplit = jk_kernel(cq.X, cq.Y, 1, cq.bucket == 0).launch != nullptr;
+            const bool cansplit = select_kernel(c, cq.X, cq.Y, 1, cq.bucket == 0).launch != nullptr;
             for (int part = 0; part < (cfg && cansplit ? 2 : 1); ++part) {
               const int prec = (cfg && part == 1) ? 1 : 0;
               a.mode = (cfg && cansplit) ? 1 + part : 0;

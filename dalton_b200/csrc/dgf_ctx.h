@@ -62,6 +62,8 @@ struct dgf_ctx {
   int cls_off[dgf::kNumPairClass + 1] = {0};
   // per class: bucket boundaries (relative to the class start), pairs sorted by (bucket, -Schwarz bin, shells)
   int bkt_off[dgf::kNumPairClass][dgf::kNumBuckets + 1] = {};
+  double cls_avg_npp[dgf::kNumPairClass] = {};  // mean primitive pairs of a class's pairs (shard cost model)
+  int cls_max_npp[dgf::kNumPairClass] = {};     // most primitive pairs of a class's pairs
   std::vector<dgf::PrimPair> pp;
   dgf::PairRec *d_pairs = nullptr;
   dgf::PrimPair *d_pp = nullptr;
@@ -70,6 +72,18 @@ struct dgf_ctx {
   int cap_slots = 0, cap_io = 0;
   double *d_D = nullptr, *d_Ds = nullptr, *d_Fh = nullptr, *d_io = nullptr;
   float *d_dmax = nullptr;
+  // Dalton blocks and the density screen on them: block of each AO shell
+  // and working shell (ws_blk_flag with kWholeBlock where the shell is its
+  // whole block), each block's first AO function and function count; device
+  // block Schwarz factors (nblk^2, built at the first screened call), block
+  // info (ao0 | nf) and block density maxima ((1 + cap_blk_slots) x nblk^2)
+  int nblk = 0;
+  std::vector<int> sh_blk, ws_blk, ws_blk_flag, blk_ao0, blk_nf;
+  double *d_blk_gab = nullptr;
+  int *d_blk_info = nullptr;
+  float *d_blk_dmax = nullptr;
+  int cap_blk_slots = 0;
+  int tile_enabled = 1;          // tiled digestion of the thread kernels (DGF_NO_TILE=1 turns it off)
   unsigned long long *d_cnt = nullptr;  // kCounterSlots x 4 per-launch counters
   // quartet plan, cached by Schwarz threshold
   double plan_thrs = -1.0;

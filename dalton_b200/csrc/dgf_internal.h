@@ -83,8 +83,9 @@ struct __align__(16) PairRec {
   double Q;        // Schwarz factor sqrt(max |(ab|ab)|)
   int64_t dbase;   // offset of the molecule's N x N block in packed D/F storage (0 for one molecule)
   int atA, atB;    // atoms of A and B
-  int pad0, pad1;
+  int blkA, blkB;  // Dalton blocks of A and B, bit kWholeBlock set when the shell is its whole block
 };
+constexpr int kWholeBlock = 1 << 30;
 
 static_assert(sizeof(PrimPair) == 96 && sizeof(PairRec) == 64, "pair records are read 16 bytes at a time");
 
@@ -121,6 +122,22 @@ struct JKArgs {
   int mode;                 // 0: all, 1: bound >= split only, 2: bound < split only
   double *diag_out;         // Schwarz mode: sqrt(max |(ab|ab)|) per bra pair, no digestion
   unsigned long long *counters;  // [0] quartets done, [1] primitive quartets, [2] skipped
+  // Dalton's density screen on its blocks (an atom's shell of angular
+  // momentum l with all its contracted functions; every working shell lies
+  // in one): block Schwarz factors GAB (nblk x nblk), block maxima of |D| of
+  // the AO densities, over all slots and per slot (blk_stride apart), the
+  // ICEDIF threshold (0: off) and bits.  blk_gab null: no density screen.
+  const double *blk_gab;
+  const float *blk_dmax;
+  const float *blk_dmax_slot;
+  int64_t blk_stride;
+  int nblk;
+  double ice_thr;
+  int icedif;
+  // tiled digestion (thread kernels, one density slot, one molecule): the
+  // tile holds tile_fa rows of A and the rows of B of the block's bra pair,
+  // tile_n columns each, in dynamic shared memory; tile_rows = 0: no tile
+  int tile_rows, tile_fa, tile_n;
   // gradient mode (dgf_grad2e): densities D1, D2 (N*N) and grad (natom*3)
   const double *G1, *G2;
   double *grad;
@@ -138,25 +155,39 @@ __host__ __device__ inline int sph_offset(int l) {
 constexpr int kSphTableDoubles = 1 * 1 + 3 * 3 + 5 * 6 + 7 * 10 + 9 * 15;
 
 typedef void (*JKLauncher)(const JKArgs &, int grid, int block, size_t smem, cudaStream_t);
+// Resident blocks per SM of a kernel with `smem` bytes of dynamic shared memory.
+typedef int (*JKOccupancy)(size_t smem);
+
+enum { kKindThread = 0, kKindTeam = 1, kKindWarpTeam = 2, kKindWarp = 4 };
 
 struct ClassKernel {
   JKLauncher launch;
   int block;
-  size_t smem;   // dynamic shared memory (team kernels); 0 for thread kernels
+  size_t smem;   // dynamic shared memory (team kernels); 0 for thread kernels (plus the tile when tiled)
   int chunks;    // thread kernels: A-component chunks (grid.y)
   int qpb;       // quartets a block works on at a time (grid sizing)
+  int kind;      // kKindThread, kKindTeam, kKindWarpTeam or kKindWarp
+  JKOccupancy occ;  // thread kernels: occupancy query for tiled launches
 };
+
+// Tiled digestion of the thread kernels: largest tile (bytes of dynamic
+// shared memory), and the fewest quartets per bra pair for which a launch
+// uses it (the tile is flushed once per bra pair and block).
+constexpr size_t kTileMaxBytes = 96 * 1024;
+constexpr int64_t kTileMinQuartetsPerBra = 256;
 
 constexpr int kThreadVariants = 2;
 
 // Per-class launch table (filled by dgf_jk.cu): index [X][Y] of pair classes.
-// precision: 0 = default FP64 kernel, 1 = FP32 thread kernel, 2 = team kernel.
+// precision: 0 = default FP64 kernel, 1 = FP32 kernel, 2 = team kernel.
 // ket1: the launch's kets have one primitive pair each (thread kernels then
-// use their single-ket-primitive form).
-const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1 = false);
-// variant -2 = warp-team kernel, -1 = team kernel, >= 0 = thread-kernel
-// variant (precision 0/1).
-const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1 = false);
+// use their single-ket-primitive form); bra1: so do all pairs of the bra
+// class (with ket1, the condition of the warp-per-quartet kernel).
+const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1 = false, bool bra1 = false);
+// variant -3 = warp-per-quartet kernel, -2 = warp-team kernel, -1 = team
+// kernel, >= 0 = thread-kernel variant (precision 0/1).
+const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1 = false,
+                                     bool bra1 = false);
 cudaError_t jk_prepare_all();
 
 void boys_table_host(std::vector<double> &out);       // [kBoysMaxM+1][kBoysTableDoubles]

@@ -10,38 +10,43 @@ namespace dgf {
 JKEntry g_jk_table[kNumPairClass][kNumPairClass];
 
 namespace {
-const ClassKernel kNone{nullptr, 0, 0, 0, 0};
+const ClassKernel kNone{nullptr, 0, 0, 0, 0, 0, nullptr};
 }
 
-// variant: -2 = warp-team kernel, -1 = team kernel, 0.. = thread-kernel variant; precision 0 = FP64,
-// 1 = FP32.  Returns a kernel with launch == nullptr when absent.
-const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1) {
+// variant: -3 = warp-per-quartet kernel, -2 = warp-team kernel, -1 = team
+// kernel, 0.. = thread-kernel variant; precision 0 = FP64, 1 = FP32.
+// Returns a kernel with launch == nullptr when absent.
+const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1, bool bra1) {
   const JKEntry &e = g_jk_table[X][Y];
+  const int p = precision ? 1 : 0;
+  if (variant == -3) return (ket1 && bra1) ? e.warp[p] : kNone;
   if (variant == -2) return precision == 0 ? e.wteam : kNone;
   if (variant < 0) return precision == 0 ? e.team : kNone;
   if (variant >= kThreadVariants) return kNone;
-  const int p = precision ? 1 : 0;
   if (ket1 && e.thr1[p][variant].launch) return e.thr1[p][variant];
   return e.thr[p][variant];
 }
 
-// Default choice: first thread variant when the class has one, else team.
-const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1) {
+// Default choice: first thread variant when the class has one, else the
+// warp-per-quartet kernel for single-primitive launches, else team.
+const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1, bool bra1) {
   const JKEntry &e = g_jk_table[X][Y];
   if (precision == 2) return e.team;
   const int p = precision == 1 ? 1 : 0;
   if (ket1 && e.thr1[p][0].launch) return e.thr1[p][0];
-  if (precision == 1) return e.thr[1][0];
-  return e.thr[0][0].launch ? e.thr[0][0] : e.team;
+  if (e.thr[p][0].launch) return e.thr[p][0];
+  if (ket1 && bra1 && e.warp[p].launch) return e.warp[p];
+  return precision == 1 ? kNone : e.team;
 }
 
 cudaError_t jk_prepare_all() {
   for (int X = 0; X < kNumPairClass; ++X)
-    for (int Y = 0; Y <= X; ++Y) {
-      if (!g_jk_table[X][Y].prepare) return cudaErrorInitializationError;
-      cudaError_t e = g_jk_table[X][Y].prepare();
-      if (e != cudaSuccess) return e;
-    }
+    for (int Y = 0; Y <= X; ++Y)
+      for (int P = 0; P < 3; ++P) {
+        if (!g_jk_table[X][Y].prepare[P]) return cudaErrorInitializationError;  // a generated part is missing
+        cudaError_t e = g_jk_table[X][Y].prepare[P]();
+        if (e != cudaSuccess) return e;
+      }
   return cudaSuccess;
 }
 

@@ -22,12 +22,51 @@
 
 namespace dgf {
 
+// Segmented sum over runs of adjacent lanes with equal keys: after the call
+// the first lane of each run (its head) holds the run's sum.  `end` is the
+// last lane of the calling lane's run (seg_end below).
+__device__ __forceinline__ double seg_sum(double v, int lane, int end) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double t = __shfl_down_sync(0xffffffffu, v, off);
+    if (lane + off <= end) v += t;
+  }
+  return v;
+}
+
+// Runs of adjacent lanes with equal key: whether this lane starts a run and
+// the last lane of its run.
+__device__ __forceinline__ void seg_end(int key, int lane, bool &head, int &end) {
+  const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+  head = (lane == 0) || prev != key;
+  const unsigned hm = __ballot_sync(0xffffffffu, head);
+  const unsigned after = hm & ~((2u << lane) - 1u);
+  end = after ? __ffs(after) - 2 : 31;
+}
+
 // Digestion of one quartet block g[FA][FB][FC][FD] (FA rows of A starting at
-// function a_off): J_ab (warp-reduced when the warp shares its bra pair),
-// J_cd, K_ac, K_ad, K_bc, K_bd as FP64 atomics into the half Fock matrices.
+// function a_off) into the half Fock matrices with FP64 atomics: the six J/K
+// blocks of FCKCON (DALTON/abacus/herfckcon.F:66-80)
+//   J_ab += g Ds_cd,  J_cd += g Ds_ab,
+//   K_ac += g D_bd, K_ad += g D_bc, K_bc += g D_ad, K_bd += g D_ac.
+// The lanes whose bra pair is the group bra (the block's tile bra, or the
+// warp's first bra without a tile) sum J_ab with a warp reduction and K_ac,
+// K_bc over runs of adjacent lanes with the same C shell (the kets of a
+// Schwarz bin are sorted by shell) with a segmented reduction, so that one
+// atomic serves the run.  The exchange blocks read the density rows of the
+// bra's functions; with a tile those rows come from shared memory (loaded
+// once per bra pair and block), else from global memory.  Density screening
+// per density (ICEDIF, DALTON/abacus/her2fck.F:221-222,446-466): with
+// ice_thr > 0, a lane whose quartet consists of whole Dalton blocks drops
+// its Coulomb part of density k when max(|D|_AB,|D|_CD) max|g| < ice_thr
+// (bit 1 of icedif) and its exchange part when the exchange blocks' bound
+// does (bit 2), with the block maxima of the AO density.
 template <int FA, int FB, int FC, int FD>
-__device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool work, bool uniform, int ib, int ic,
-                                          int ib0, const PairRec &br, const PairRec &kt, int a_off) {
+__device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool work, int ib, int ic, int gib,
+                                          const PairRec &br, const PairRec &kt, int a_off, const double *dtile,
+                                          int tile_fa) {
+  // Segmented reduction of K_ac and K_bc where it is cheap next to the atomics it saves.
+  constexpr bool SEG = (FA + FB) * FC <= 18;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   double w = 0.0;
@@ -37,25 +76,58 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
     if (kt.same) w *= 0.5;
     if (a.same_class && ib == ic + a.ket_off) w *= 0.5;
   }
-  // The warp's bra pair (valid on every lane) for the warp-reduced J_ab block;
-  // a quartet's bra and ket belong to one molecule, so its N x N block is
-  // the bra's.
-  const PairRec brw = load_pair_fock(a.bra + ib0);
-  const int N = work ? br.nbfm : brw.nbfm;
-  const int64_t db = work ? br.dbase : brw.dbase;
+  // Group: lanes on the group bra reduce their bra-row blocks together.
+  const bool grp = work && ib == gib;
+  const PairRec brg = load_pair_fock(a.bra + gib);
+  const double *dt = grp ? dtile : nullptr;  // the density tile serves group lanes only
+  const int tn = brg.nbfm;
+  // Runs of group lanes with the same C shell (K_ac, K_bc); other lanes are runs of their own.
+  bool head = true;
+  int send = lane;
+  if (SEG) seg_end(grp ? kt.aoA : -1 - lane, lane, head, send);
+  double aomax = 0.0;
+  bool ice = false;
+  if (a.ice_thr > 0.0 && work) {
+    const int4 bb = block_of_pair(a.bra + ib), kb = block_of_pair(a.ket + ic);
+    ice = (bb.z & bb.w & kb.z & kb.w) != 0;  // all four shells are whole Dalton blocks
+    if (ice) {
+#pragma unroll
+      for (int e = 0; e < FA * FB * FC * FD; ++e) aomax = fmax(aomax, fabs(g[e]));
+    }
+  }
+  const int N = work ? br.nbfm : brg.nbfm;
+  const int64_t db = work ? br.dbase : brg.dbase;
   for (int k = 0; k < a.nslot; ++k) {
     const double *Dk = a.D + k * a.slot_stride + db;
     const double *Dsk = a.Ds + k * a.slot_stride + db;
     double *Fk = a.Fh + k * a.slot_stride + db;
-    double *Fw = a.Fh + k * a.slot_stride + brw.dbase;
-    const double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
+    double *Fg = a.Fh + k * a.slot_stride + brg.dbase;
+    // Rows of the bra's functions in D: the tile (slot 0 only) or global memory.
+    auto dA = [&](int x, int col) -> double {
+      return dt ? dt[(size_t)(a_off + x) * tn + col] : Dk[(size_t)(br.aoA + a_off + x) * N + col];
+    };
+    auto dB = [&](int y, int col) -> double {
+      return dt ? dt[(size_t)(tile_fa + y) * tn + col] : Dk[(size_t)(br.aoB + y) * N + col];
+    };
+    double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
+    if (ice) {
+      const int4 bb = block_of_pair(a.bra + ib), kb = block_of_pair(a.ket + ic);
+      const float *dm = a.blk_dmax_slot + k * a.blk_stride;
+      const int n = a.nblk;
+      const double dj = fmaxf(dm[bb.x * n + bb.y], dm[kb.x * n + kb.y]);
+      const double dk = fmaxf(fmaxf(dm[bb.x * n + kb.x], dm[bb.x * n + kb.y]),
+                              fmaxf(dm[bb.y * n + kb.x], dm[bb.y * n + kb.y]));
+      if ((a.icedif & 1) && dj * aomax < a.ice_thr) js = 0.0;
+      if ((a.icedif & 2) && dk * aomax < a.ice_thr) ks = 0.0;
+    }
     if (a.jscale[k] != 0.0) {
+      // J_ab: group lanes warp-reduced, others per lane
 #pragma unroll
       for (int x = 0; x < FA; ++x)
 #pragma unroll
         for (int y = 0; y < FB; ++y) {
           double s = 0.0;
-          if (work) {
+          if (work && js != 0.0) {
 #pragma unroll
             for (int c = 0; c < FC; ++c)
 #pragma unroll
@@ -63,15 +135,14 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
                 s += g[((x * FB + y) * FC + c) * FD + d] * Dsk[(size_t)(kt.aoA + c) * N + kt.aoB + d];
             s *= js;
           }
-          if (uniform) {
+          double r = grp ? s : 0.0;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(full, s, off);
-            if (lane == 0) atomicAdd(Fw + (size_t)(brw.aoA + a_off + x) * brw.nbfm + brw.aoB + y, s);
-          } else if (work) {
-            atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + br.aoB + y, s);
-          }
+          for (int off = 16; off > 0; off >>= 1) r += __shfl_xor_sync(full, r, off);
+          if (lane == 0 && r != 0.0) atomicAdd(Fg + (size_t)(brg.aoA + a_off + x) * brg.nbfm + brg.aoB + y, r);
+          if (work && !grp && s != 0.0) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + br.aoB + y, s);
         }
-      if (work) {
+      // J_cd: per lane
+      if (work && js != 0.0) {
 #pragma unroll
         for (int c = 0; c < FC; ++c)
 #pragma unroll
@@ -86,50 +157,71 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
           }
       }
     }
-    if (work && a.kscale[k] != 0.0) {
+    if (a.kscale[k] != 0.0) {
+      const bool kw = work && ks != 0.0;
 #pragma unroll
       for (int x = 0; x < FA; ++x) {
+        // K_ac: runs of equal C reduced, the run's head adds
 #pragma unroll
         for (int c = 0; c < FC; ++c) {
           double s = 0.0;
+          if (kw) {
 #pragma unroll
-          for (int y = 0; y < FB; ++y)
+            for (int y = 0; y < FB; ++y)
 #pragma unroll
-            for (int d = 0; d < FD; ++d)
-              s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoB + y) * N + kt.aoB + d];
-          atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, ks * s);
+              for (int d = 0; d < FD; ++d) s += g[((x * FB + y) * FC + c) * FD + d] * dB(y, kt.aoB + d);
+            s *= ks;
+          }
+          if (SEG) {
+            const double r = seg_sum(grp ? s : 0.0, lane, send);
+            if (grp && head && r != 0.0) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, r);
+            if (kw && !grp) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, s);
+          } else if (kw) {
+            atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, s);
+          }
         }
+        // K_ad: per lane
 #pragma unroll
         for (int d = 0; d < FD; ++d) {
+          if (!kw) continue;
           double s = 0.0;
 #pragma unroll
           for (int y = 0; y < FB; ++y)
 #pragma unroll
-            for (int c = 0; c < FC; ++c)
-              s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoB + y) * N + kt.aoA + c];
+            for (int c = 0; c < FC; ++c) s += g[((x * FB + y) * FC + c) * FD + d] * dB(y, kt.aoA + c);
           atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoB + d, ks * s);
         }
       }
 #pragma unroll
       for (int y = 0; y < FB; ++y) {
+        // K_bc: runs of equal C reduced
 #pragma unroll
         for (int c = 0; c < FC; ++c) {
           double s = 0.0;
+          if (kw) {
 #pragma unroll
-          for (int x = 0; x < FA; ++x)
+            for (int x = 0; x < FA; ++x)
 #pragma unroll
-            for (int d = 0; d < FD; ++d)
-              s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoA + a_off + x) * N + kt.aoB + d];
-          atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, ks * s);
+              for (int d = 0; d < FD; ++d) s += g[((x * FB + y) * FC + c) * FD + d] * dA(x, kt.aoB + d);
+            s *= ks;
+          }
+          if (SEG) {
+            const double r = seg_sum(grp ? s : 0.0, lane, send);
+            if (grp && head && r != 0.0) atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, r);
+            if (kw && !grp) atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, s);
+          } else if (kw) {
+            atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, s);
+          }
         }
+        // K_bd: per lane
 #pragma unroll
         for (int d = 0; d < FD; ++d) {
+          if (!kw) continue;
           double s = 0.0;
 #pragma unroll
           for (int x = 0; x < FA; ++x)
 #pragma unroll
-            for (int c = 0; c < FC; ++c)
-              s += g[((x * FB + y) * FC + c) * FD + d] * Dk[(size_t)(br.aoA + a_off + x) * N + kt.aoA + c];
+            for (int c = 0; c < FC; ++c) s += g[((x * FB + y) * FC + c) * FD + d] * dA(x, kt.aoA + c);
           atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoB + d, ks * s);
         }
       }
@@ -137,13 +229,30 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
   }
 }
 
-constexpr int kThreadBlock = 128;
+// Loads the density rows of bra `ib` (rows of A, then rows of B, tile_n
+// columns each, density slot 0) into the tile; every thread of the block
+// takes part, reading whole rows.
+__device__ __forceinline__ void tile_load(const JKArgs &a, double *tile, int rows, int fa, int ib) {
+  const PairRec br = load_pair_fock(a.bra + ib);
+  const int n = br.nbfm;
+  const double *D = a.D + br.dbase;
+  for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
+    const int r = e / n, col = e - r * n;
+    const int row = r < fa ? br.aoA + r : br.aoB + (r - fa);
+    tile[e] = __ldg(D + (size_t)row * n + col);
+  }
+}
+
+constexpr int kThreadBlock = 256;
 constexpr int kThreadWarps = kThreadBlock / 32;
+// 32-quartet chunks each warp processes between two block synchronisations
+// of the tiled form.
+constexpr int kChunksPerSync = 2;
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, const double *sph, Tc *ebra,
-                                               unsigned long long &cnt_q, unsigned long long &cnt_p,
-                                               unsigned long long &cnt_s) {
+                                               double *tile, int *s_tib, unsigned long long &cnt_q,
+                                               unsigned long long &cnt_p, unsigned long long &cnt_s) {
   constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr int A0 = CH * NA / CA, A1 = (CH + 1) * NA / CA, NAc = A1 - A0;  // this chunk's A components
@@ -157,27 +266,64 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
   constexpr int NOUT = cmax(NACC, cmax(FAc, NAc) * cmax(NB, FBc) * cmax(NC, FCc) * cmax(ND, FDc));
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
-  // Each warp takes one contiguous range of the queue (a multiple of 32
-  // quartets), so its bra index only moves forward: one binary search per
-  // warp, then a short walk along qoff per 32 quartets.
-  const int64_t nwarp = (int64_t)gridDim.x * (blockDim.x >> 5);
-  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int64_t span = (((a.nquartet - a.q_begin) + nwarp - 1) / nwarp + 31) & ~(int64_t)31;
-  const int64_t wbegin = a.q_begin + wid * span, wend = min(wbegin + span, a.nquartet);
-  int ibw = 0;
-  if (wbegin < wend && lane == 0) ibw = find_bra(a.qoff, a.nbra, wbegin);
-  ibw = __shfl_sync(full, ibw, 0);
-  for (int64_t base = wbegin; base < wend; base += 32) {
+  // Each block takes one contiguous range of the queue; its warps work on
+  // consecutive 32-quartet chunks of it, kChunksPerSync chunks per warp per
+  // block iteration, so that the block stays on one bra pair for long runs
+  // (the tile of its bra rows).  A warp's chunks only move forward, so its
+  // bra index is found once by binary search and then by a short walk along
+  // qoff.
+  const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  const int64_t iter = (int64_t)32 * nw * kChunksPerSync;
+  const int64_t nq = a.nquartet - a.q_begin;
+  const int64_t bspan = ((nq + gridDim.x - 1) / gridDim.x + 31) & ~(int64_t)31;
+  const int64_t bbegin = a.q_begin + (int64_t)blockIdx.x * bspan, bend = min(bbegin + bspan, a.nquartet);
+  const bool use_tile = tile != nullptr;
+  int ibw = -1;              // the warp's running bra
+  int tile_ib = -1, tib = -1;  // the block's tile bra; thread 0's running search for it
+  int parity = 0;
+  for (int64_t ibase = bbegin; ibase < bend; ibase += iter) {
+    if (use_tile) {
+      // Tile bra of this iteration: the bra of its last quartet (runs usually continue into the next one).
+      if (threadIdx.x == 0) {
+        const int64_t ql = min(ibase + iter, bend) - 1;
+        if (tib < 0) {
+          tib = find_bra(a.qoff, a.nbra, ql);
+        } else {
+          int steps = 0;
+          while (ql >= a.qoff[tib + 1] && steps < 32) {
+            ++tib;
+            ++steps;
+          }
+          if (ql >= a.qoff[tib + 1]) tib = find_bra(a.qoff, a.nbra, ql);
+        }
+        s_tib[parity] = tib;
+      }
+      __syncthreads();
+      const int nib = s_tib[parity];
+      parity ^= 1;
+      if (nib != tile_ib) {  // every warp has finished reading the previous tile (barrier above)
+        tile_load(a, tile, a.tile_rows, a.tile_fa, nib);
+        __syncthreads();
+        tile_ib = nib;
+      }
+    }
+    for (int jc = 0; jc < kChunksPerSync; ++jc) {
+    const int64_t base = ibase + ((int64_t)jc * nw + warp) * 32;
+    if (base >= bend) break;
     const int64_t q = base + lane;
-    const bool active = q < wend;
+    const bool active = q < bend;
     int ib0 = ibw;
     if (lane == 0) {  // the warp's first bra: a short walk, else a search
-      int steps = 0;
-      while (base >= a.qoff[ib0 + 1] && steps < 32) {
-        ++ib0;
-        ++steps;
+      if (ib0 < 0) {
+        ib0 = find_bra(a.qoff, a.nbra, base);
+      } else {
+        int steps = 0;
+        while (base >= a.qoff[ib0 + 1] && steps < 32) {
+          ++ib0;
+          ++steps;
+        }
+        if (base >= a.qoff[ib0 + 1]) ib0 = find_bra(a.qoff, a.nbra, base);
       }
-      if (base >= a.qoff[ib0 + 1]) ib0 = find_bra(a.qoff, a.nbra, base);
     }
     ib0 = __shfl_sync(full, ib0, 0);
     ibw = ib0;
@@ -196,7 +342,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
       kt = load_pair_fock(a.ket + ic);
       // K1 with a known layout: the ket's primitive pair is fetched alongside its record
       if (K1 && a.ket_pp0 >= 0) P2one = load_prim<(LC + LD > 0)>(a.pp + a.ket_pp0 + ic);
-      sel = quartet_select(a, br, kt);
+      sel = quartet_select(a, br, kt, a.bra + ib, a.ket + ic);
       if (sel == 2 && CH == 0 && a.mode != 2) ++cnt_s;  // a split class counts its skips in the FP64 launch
     }
     const bool work = active && sel == 0;
@@ -394,24 +540,25 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
       }
     }
     // Digestion with compile-time function counts (spherical or Cartesian).
-    const bool uniform = __all_sync(full, !work || ib == ib0) && __any_sync(full, work);
     if (!__any_sync(full, work)) continue;
+    const int gib = use_tile ? tile_ib : ib0;
     if (sphr)
-      jk_digest<FAc, FBc, FCc, FDc>(a, g, work, uniform, ib, ic, ib0, br, kt, 0);
+      jk_digest<FAc, FBc, FCc, FDc>(a, g, work, ib, ic, gib, br, kt, 0, tile, a.tile_fa);
     else
-      jk_digest<NAc, NB, NC, ND>(a, g, work, uniform, ib, ic, ib0, br, kt, A0);
+      jk_digest<NAc, NB, NC, ND>(a, g, work, ib, ic, gib, br, kt, A0, tile, a.tile_fa);
+    }
   }
 }
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, const double *tab, const double *sph,
-                                                   Tc *ebra, unsigned long long &q, unsigned long long &p,
-                                                   unsigned long long &s) {
+                                                   Tc *ebra, double *tile, int *s_tib, unsigned long long &q,
+                                                   unsigned long long &p, unsigned long long &s) {
   if constexpr (CH < CA) {
     if (chunk == CH)
-      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, sph, ebra, q, p, s);
+      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, sph, ebra, tile, s_tib, q, p, s);
     else
-      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, sph, ebra, q, p, s);
+      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, sph, ebra, tile, s_tib, q, p, s);
   }
 }
 
@@ -419,7 +566,7 @@ __device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, c
 // classes are latency bound (few FLOPs per quartet, long chains of dependent
 // loads), so they trade registers for warps.
 #ifndef DGF_THREAD_MINB_L2
-#define DGF_THREAD_MINB_L2 4
+#define DGF_THREAD_MINB_L2 2
 #endif
 #ifndef DGF_THREAD_MINB_L3
 #define DGF_THREAD_MINB_L3 1
@@ -436,12 +583,17 @@ __global__ void __launch_bounds__(kThreadBlock, thread_min_blocks(LA + LB + LC +
   __shared__ double tab[kBoysTableDoubles];
   __shared__ double sph[kSphTableDoubles];
   __shared__ Tc ebra_all[kThreadWarps][3 * EA];
+  __shared__ int s_tib[2];
+  // Tile of the density rows of the block's bra pair (tiled launches):
+  // tile_rows x tile_n doubles of dynamic shared memory.
+  extern __shared__ double tile_dyn[];
+  double *tile = a.tile_rows > 0 ? tile_dyn : nullptr;
   for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
   for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
   __syncthreads();
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
-  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, sph, ebra_all[threadIdx.x >> 5], cnt_q, cnt_p,
-                                                cnt_s);
+  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, sph, ebra_all[threadIdx.x >> 5], tile, s_tib,
+                                                cnt_q, cnt_p, cnt_s);
   if (a.counters) {
     const int lane = threadIdx.x & 31;
 #pragma unroll

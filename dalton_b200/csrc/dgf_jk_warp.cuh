@@ -1,0 +1,509 @@
+// Warp-per-quartet McMurchie-Davidson J/K kernel for the high angular
+// momentum classes (L = la+lb+lc+ld >= 6, up to (ff|fd)), where one thread
+// cannot hold a quartet's intermediates in registers.
+//
+// Each warp of a block works through its own contiguous range of the class
+// queue, one quartet at a time; every index pattern is known at compile
+// time and the lanes split the work of each step:
+//   R_tuv            Hermite recursion level by level in a (L+1)^3 box in
+//                    shared memory, one (t,u,v) per lane     (HERI, her2her.F)
+//   X[cd][tuv]       ket transform, one bra Hermite index tuv per lane: each
+//                    R value is read once and applied to every ket
+//                    component that uses it, with the ket's Hermite
+//                    coefficient products E^cd_{tau nu phi} from a table
+//                    built per ket primitive pair          (C2, her2el2.F)
+//   (ab|cd)          bra transform, one ket component cd per lane, each X
+//                    value read once and applied to every bra component,
+//                    with the bra's product table (kept while consecutive
+//                    quartets share the bra)               (C1, her2el1.F)
+//   spherical        bra side per lane (register block), ket side per lane
+//                    over rows                             (C1SPHR/C2SPHR)
+//   digestion        the six J/K blocks (FCKCON, herfckcon.F:66-80), one
+//                    output element per lane, FP64 atomics
+// Tc is the arithmetic type of R, the transforms and the tables (double:
+// FP64 drop-in; float: FP32 half of the mixed form); Boys function,
+// prefactor, accumulation across primitive pairs and digestion are FP64.
+#pragma once
+
+#include <utility>
+
+#include "dgf_jk_team.cuh"
+
+namespace dgf {
+namespace wq {
+
+// (t,u,v) of compact index e (tuv_index order), at compile time.
+constexpr int tuv_s(int e) {
+  int s = 0;
+  while (n3(s) <= e) ++s;
+  return s;
+}
+constexpr int tuv_w(int e) {
+  const int r = e - n3(tuv_s(e) - 1 >= 0 ? tuv_s(e) - 1 : 0) * (tuv_s(e) > 0 ? 1 : 0);
+  int w = 0;
+  while ((w + 1) * (w + 2) / 2 <= r) ++w;
+  return w;
+}
+constexpr int tuv_v(int e) {
+  const int r = e - (tuv_s(e) > 0 ? n3(tuv_s(e) - 1) : 0);
+  return r - tuv_w(e) * (tuv_w(e) + 1) / 2;
+}
+constexpr int tuv_u(int e) { return tuv_w(e) - tuv_v(e); }
+constexpr int tuv_t(int e) { return tuv_s(e) - tuv_w(e); }
+
+// Hermite terms of Cartesian component pair ij = i*ncart(lb)+j of a shell
+// pair (la, lb): (ix+jx+1)(iy+jy+1)(iz+jz+1), and their offsets in a
+// compact table ordered by ij, then t, u, v.
+constexpr int nterm(int la, int lb, int ij) {
+  const int i = ij / ncart(lb), j = ij % ncart(lb);
+  return (cart_x(la, i) + cart_x(lb, j) + 1) * (cart_y(la, i) + cart_y(lb, j) + 1) *
+         (cart_z(la, i) + cart_z(lb, j) + 1);
+}
+constexpr int term_off(int la, int lb, int ij) {
+  int off = 0;
+  for (int k = 0; k < ij; ++k) off += nterm(la, lb, k);
+  return off;
+}
+constexpr int nterm_all(int la, int lb) { return term_off(la, lb, ncart(la) * ncart(lb)); }
+// Whether component pair ij uses Hermite index (t,u,v), and the term's index.
+constexpr bool uses(int la, int lb, int ij, int t, int u, int v) {
+  const int i = ij / ncart(lb), j = ij % ncart(lb);
+  return t <= cart_x(la, i) + cart_x(lb, j) && u <= cart_y(la, i) + cart_y(lb, j) &&
+         v <= cart_z(la, i) + cart_z(lb, j);
+}
+constexpr int term_at(int la, int lb, int ij, int t, int u, int v) {
+  const int i = ij / ncart(lb), j = ij % ncart(lb);
+  const int ny = cart_y(la, i) + cart_y(lb, j) + 1, nz = cart_z(la, i) + cart_z(lb, j) + 1;
+  return term_off(la, lb, ij) + (t * ny + u) * nz + v;
+}
+
+constexpr int odd(int n) { return n | 1; }
+
+// Calls f(std::integral_constant<int, i>) for i = 0 .. N-1, so that the loop
+// index is a constant expression inside f (index arithmetic and term
+// selection at compile time).
+template <typename F, int... I>
+__device__ __forceinline__ void static_for_impl(F &&f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F &&f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// Per-warp shared memory of class (LA LB | LC LD) in units of 8 bytes.
+template <int LA, int LB, int LC, int LD, typename Tc>
+struct Shape {
+  static constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD, BOX = L + 1;
+  static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  static constexpr int NAB = NA * NB, NCD = NC * ND, N3AB = n3(LAB), N3CD = n3(LCD), N3L = n3(L);
+  static constexpr int EA = (LA + 1) * (LB + 1) * (LAB + 1), EC = (LC + 1) * (LD + 1) * (LCD + 1);
+  static constexpr int TAB = nterm_all(LA, LB), TCD = nterm_all(LC, LD);
+  static constexpr int PX = odd(N3AB);  // row stride of X[cd][tuv]
+  static constexpr int PG = odd(NCD);   // row stride of the (ab|cd) blocks
+  static constexpr int FAm = cmax(NA, LA >= 2 ? 2 * LA + 1 : NA), FBm = cmax(NB, LB >= 2 ? 2 * LB + 1 : NB);
+  static constexpr int FCm = cmax(NC, LC >= 2 ? 2 * LC + 1 : NC), FDm = cmax(ND, LD >= 2 ? 2 * LD + 1 : ND);
+  static constexpr int W = sizeof(Tc) == 8 ? 1 : 2;  // Tc values per 8-byte unit
+  // region A: the two R boxes, later the Cartesian (ab|cd) block and the final block
+  static constexpr int RA = cmax((2 * BOX * BOX * BOX + W - 1) / W, NAB * PG);
+  // region B: X, later the block with spherical bra functions
+  static constexpr int RB = cmax((NCD * PX + W - 1) / W, NAB * PG);
+  // Hermite 1D tables and product tables of bra and ket (Tc)
+  static constexpr int RT = (3 * EA + 3 * EC + TAB + TCD + W - 1) / W;
+  // six density blocks (double)
+  static constexpr int RD = FAm * FBm + FCm * FDm + FAm * FCm + FAm * FDm + FBm * FCm + FBm * FDm;
+  static constexpr int PER_WARP = RA + RB + RT + RD + 8;
+  // block-wide: Boys and spherical tables, packed (t,u,v), offsets of the product tables
+  static constexpr int COMMON = kBoysTableDoubles + kSphTableDoubles + (N3L + 1) / 2;
+  static constexpr size_t smem(int warps) { return ((size_t)COMMON + (size_t)warps * PER_WARP) * 8; }
+  // warps per block: four when they fit in 100 KB, else two, else one
+  static constexpr int WPB = smem(4) <= 100 * 1024 ? 4 : smem(2) <= 100 * 1024 ? 2 : 1;
+};
+
+// Cartesian -> spherical transform of one index of a register block
+// g[PRE][N][POST] -> o[PRE][M][POST], rows m of T (M x N) at T.
+template <int PRE, int N, int M, int POST>
+__device__ __forceinline__ void sph_index(const double *g, double *o, const double *T) {
+#pragma unroll
+  for (int i = 0; i < PRE; ++i)
+#pragma unroll
+    for (int m = 0; m < M; ++m)
+#pragma unroll
+      for (int j = 0; j < POST; ++j) {
+        double s = 0.0;
+#pragma unroll
+        for (int n = 0; n < N; ++n) s += T[m * N + n] * g[(i * N + n) * POST + j];
+        o[(i * M + m) * POST + j] = s;
+      }
+}
+
+}  // namespace wq
+
+// Post-processing and digestion of the Cartesian block Gc[ab][cd] (row
+// stride PG) of one quartet: spherical transform (SPH), then the six J/K
+// blocks.  Gs and Gf are scratch blocks of the warp; Db the density blocks.
+template <int LA, int LB, int LC, int LD, typename Tc, bool SPH>
+__device__ __forceinline__ void wq_finish(const JKArgs &a, double *Gc, double *Gs, double *Gf, double *Db,
+                                          const double *sph, const PairRec &br, const PairRec &kt, int ib, int ic,
+                                          double w, int lane) {
+  using S = wq::Shape<LA, LB, LC, LD, Tc>;
+  constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NCD = S::NCD, PG = S::PG;
+  constexpr int FA = (SPH && LA >= 2) ? 2 * LA + 1 : NA, FB = (SPH && LB >= 2) ? 2 * LB + 1 : NB;
+  constexpr int FC = (SPH && LC >= 2) ? 2 * LC + 1 : NC, FD = (SPH && LD >= 2) ? 2 * LD + 1 : ND;
+  constexpr int FAB = FA * FB, FCD = FC * FD;
+  const double *G = Gc;
+  if (SPH) {
+    // bra side: one ket component cd per lane, Gc column -> Gs column
+    for (int cd = lane; cd < NCD; cd += 32) {
+      double g[NA * NB], t1[FA * NB], t2[FA * FB];
+#pragma unroll
+      for (int ab = 0; ab < NA * NB; ++ab) g[ab] = Gc[ab * PG + cd];
+      if (LA >= 2)
+        wq::sph_index<1, NA, FA, NB>(g, t1, sph + sph_offset(LA));
+      else
+#pragma unroll
+        for (int k = 0; k < NA * NB; ++k) t1[k] = g[k];
+      if (LB >= 2)
+        wq::sph_index<FA, NB, FB, 1>(t1, t2, sph + sph_offset(LB));
+      else
+#pragma unroll
+        for (int k = 0; k < FA * NB; ++k) t2[k] = t1[k];
+#pragma unroll
+      for (int ab = 0; ab < FAB; ++ab) Gs[ab * PG + cd] = t2[ab];
+    }
+    __syncwarp();
+    // ket side: one spherical bra row per lane, Gs row -> Gf row
+    for (int ab = lane; ab < FAB; ab += 32) {
+      double h[NC * ND], t1[FC * ND], t2[FC * FD];
+#pragma unroll
+      for (int cd = 0; cd < NCD; ++cd) h[cd] = Gs[ab * PG + cd];
+      if (LC >= 2)
+        wq::sph_index<1, NC, FC, ND>(h, t1, sph + sph_offset(LC));
+      else
+#pragma unroll
+        for (int k = 0; k < NC * ND; ++k) t1[k] = h[k];
+      if (LD >= 2)
+        wq::sph_index<FC, ND, FD, 1>(t1, t2, sph + sph_offset(LD));
+      else
+#pragma unroll
+        for (int k = 0; k < FC * ND; ++k) t2[k] = t1[k];
+#pragma unroll
+      for (int cd = 0; cd < FCD; ++cd) Gf[ab * PG + cd] = t2[cd];
+    }
+    __syncwarp();
+    G = Gf;
+  }
+  // Largest integral for the per-density Coulomb/exchange screen (ICEDIF).
+  bool ice = false;
+  double aomax = 0.0;
+  if (a.ice_thr > 0.0) {
+    const int4 bb = block_of_pair(a.bra + ib), kb = block_of_pair(a.ket + ic);
+    ice = (bb.z & bb.w & kb.z & kb.w) != 0;
+    if (ice) {
+      for (int e = lane; e < FAB * FCD; e += 32) aomax = fmax(aomax, fabs(G[(e / FCD) * PG + e % FCD]));
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) aomax = fmax(aomax, __shfl_xor_sync(0xffffffffu, aomax, off));
+    }
+  }
+  const int aoA = br.aoA, aoB = br.aoB, aoC = kt.aoA, aoD = kt.aoB;
+  const int N = kt.nbfm;
+  double *Dab = Db, *Dcd = Dab + FAB, *Dac = Dcd + FCD, *Dad = Dac + FA * FC, *Dbc = Dad + FA * FD,
+         *Dbd = Dbc + FB * FC;
+  for (int k = 0; k < a.nslot; ++k) {
+    const double *Dk = a.D + k * a.slot_stride + kt.dbase;
+    const double *Dsk = a.Ds + k * a.slot_stride + kt.dbase;
+    double *Fk = a.Fh + k * a.slot_stride + kt.dbase;
+    double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
+    if (ice) {
+      const int4 bb = block_of_pair(a.bra + ib), kb = block_of_pair(a.ket + ic);
+      const float *dm = a.blk_dmax_slot + k * a.blk_stride;
+      const int n = a.nblk;
+      const double dj = fmaxf(dm[bb.x * n + bb.y], dm[kb.x * n + kb.y]);
+      const double dk = fmaxf(fmaxf(dm[bb.x * n + kb.x], dm[bb.x * n + kb.y]),
+                              fmaxf(dm[bb.y * n + kb.x], dm[bb.y * n + kb.y]));
+      if ((a.icedif & 1) && dj * aomax < a.ice_thr) js = 0.0;
+      if ((a.icedif & 2) && dk * aomax < a.ice_thr) ks = 0.0;
+    }
+    if (js == 0.0 && ks == 0.0) continue;
+    // density blocks
+    for (int e = lane; e < FAB; e += 32) Dab[e] = Dsk[(size_t)(aoA + e / FB) * N + aoB + e % FB];
+    for (int e = lane; e < FCD; e += 32) Dcd[e] = Dsk[(size_t)(aoC + e / FD) * N + aoD + e % FD];
+    for (int e = lane; e < FA * FC; e += 32) Dac[e] = Dk[(size_t)(aoA + e / FC) * N + aoC + e % FC];
+    for (int e = lane; e < FA * FD; e += 32) Dad[e] = Dk[(size_t)(aoA + e / FD) * N + aoD + e % FD];
+    for (int e = lane; e < FB * FC; e += 32) Dbc[e] = Dk[(size_t)(aoB + e / FC) * N + aoC + e % FC];
+    for (int e = lane; e < FB * FD; e += 32) Dbd[e] = Dk[(size_t)(aoB + e / FD) * N + aoD + e % FD];
+    __syncwarp();
+    if (js != 0.0) {
+      for (int e = lane; e < FAB; e += 32) {  // J_ab
+        const double *row = G + e * PG;
+        double s = 0.0;
+#pragma unroll
+        for (int cd = 0; cd < FCD; ++cd) s += row[cd] * Dcd[cd];
+        atomicAdd(Fk + (size_t)(aoA + e / FB) * N + aoB + e % FB, js * s);
+      }
+      for (int e = lane; e < FCD; e += 32) {  // J_cd
+        double s = 0.0;
+#pragma unroll
+        for (int ab = 0; ab < FAB; ++ab) s += G[ab * PG + e] * Dab[ab];
+        atomicAdd(Fk + (size_t)(aoC + e / FD) * N + aoD + e % FD, js * s);
+      }
+    }
+    if (ks != 0.0) {
+      for (int e = lane; e < FA * FC; e += 32) {  // K_ac = sum_bd g D_bd
+        const int x = e / FC, c = e % FC;
+        double s = 0.0;
+#pragma unroll
+        for (int y = 0; y < FB; ++y)
+#pragma unroll
+          for (int d = 0; d < FD; ++d) s += G[(x * FB + y) * PG + c * FD + d] * Dbd[y * FD + d];
+        atomicAdd(Fk + (size_t)(aoA + x) * N + aoC + c, ks * s);
+      }
+      for (int e = lane; e < FA * FD; e += 32) {  // K_ad = sum_bc g D_bc
+        const int x = e / FD, d = e % FD;
+        double s = 0.0;
+#pragma unroll
+        for (int y = 0; y < FB; ++y)
+#pragma unroll
+          for (int c = 0; c < FC; ++c) s += G[(x * FB + y) * PG + c * FD + d] * Dbc[y * FC + c];
+        atomicAdd(Fk + (size_t)(aoA + x) * N + aoD + d, ks * s);
+      }
+      for (int e = lane; e < FB * FC; e += 32) {  // K_bc = sum_ad g D_ad
+        const int y = e / FC, c = e % FC;
+        double s = 0.0;
+#pragma unroll
+        for (int x = 0; x < FA; ++x)
+#pragma unroll
+          for (int d = 0; d < FD; ++d) s += G[(x * FB + y) * PG + c * FD + d] * Dad[x * FD + d];
+        atomicAdd(Fk + (size_t)(aoB + y) * N + aoC + c, ks * s);
+      }
+      for (int e = lane; e < FB * FD; e += 32) {  // K_bd = sum_ac g D_ac
+        const int y = e / FD, d = e % FD;
+        double s = 0.0;
+#pragma unroll
+        for (int x = 0; x < FA; ++x)
+#pragma unroll
+          for (int c = 0; c < FC; ++c) s += G[(x * FB + y) * PG + c * FD + d] * Dac[x * FC + c];
+        atomicAdd(Fk + (size_t)(aoB + y) * N + aoD + d, ks * s);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Compact table of Hermite coefficient products of a shell pair (la, lb):
+// for every Cartesian component pair ij and (t,u,v) it uses,
+// E_x[ix,jx,t] E_y[iy,jy,u] E_z[iz,jz,v] from the 1D tables E (3 x EN),
+// at wq::term_at; one component pair per lane.
+template <int LA, int LB, typename Tc>
+__device__ __forceinline__ void wq_product_table(const Tc *E, Tc *tab, int lane) {
+  constexpr int NB = ncart(LB), NIJ = ncart(LA) * NB, LT = LA + LB + 1, EN = (LA + 1) * (LB + 1) * LT;
+  for (int ij = lane; ij < NIJ; ij += 32) {
+    int ix, iy, iz, jx, jy, jz;
+    cart_decode(LA, ij / NB, ix, iy, iz);
+    cart_decode(LB, ij % NB, jx, jy, jz);
+    int off = 0;
+    for (int k = 0; k < ij; ++k) {
+      int ax, ay, az, bx, by, bz;
+      cart_decode(LA, k / NB, ax, ay, az);
+      cart_decode(LB, k % NB, bx, by, bz);
+      off += (ax + bx + 1) * (ay + by + 1) * (az + bz + 1);
+    }
+    const Tc *ex = E + (ix * (LB + 1) + jx) * LT, *ey = E + EN + (iy * (LB + 1) + jy) * LT,
+             *ez = E + 2 * EN + (iz * (LB + 1) + jz) * LT;
+    for (int t = 0; t <= ix + jx; ++t)
+      for (int u = 0; u <= iy + jy; ++u) {
+        const Tc exy = ex[t] * ey[u];
+        for (int v = 0; v <= iz + jz; ++v) tab[off++] = exy * ez[v];
+      }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename Tc>
+__global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
+  using S = wq::Shape<LA, LB, LC, LD, Tc>;
+  constexpr int L = S::L, LAB = S::LAB, BOX = S::BOX, NAB = S::NAB, NCD = S::NCD, N3AB = S::N3AB,
+                N3CD = S::N3CD, N3L = S::N3L, EA = S::EA, EC = S::EC, PX = S::PX, PG = S::PG;
+  extern __shared__ double sm[];
+  double *tab = sm;
+  double *sph = tab + kBoysTableDoubles;
+  int *tuvt = (int *)(sph + kSphTableDoubles);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  double *wbase = sm + S::COMMON + (size_t)warp * S::PER_WARP;
+  double *regA = wbase, *regB = regA + S::RA;
+  Tc *Eb = (Tc *)(regB + S::RB), *Ek = Eb + 3 * EA, *Tb = Ek + 3 * EC, *Tk = Tb + S::TAB;
+  double *Db = regB + S::RB + S::RT;
+  Tc *R0 = (Tc *)regA, *R1 = R0 + BOX * BOX * BOX;
+  Tc *X = (Tc *)regB;
+  double *Gc = regA, *Gs = regB, *Gf = regA;
+
+  for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
+  for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
+  for (int e = threadIdx.x; e < N3L; e += blockDim.x) {
+    int t, u, v;
+    tuv_decode(e, t, u, v);
+    tuvt[e] = (t * BOX + u) * BOX + v;  // position of (t,u,v) in the R box
+  }
+  __syncthreads();
+  unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
+  // One contiguous range of the queue per warp.
+  const int64_t nteam = (int64_t)gridDim.x * nw, team = (int64_t)blockIdx.x * nw + warp;
+  const int64_t span = (a.nquartet - a.q_begin + nteam - 1) / nteam;
+  const int64_t qbeg = a.q_begin + team * span, qend = min(qbeg + span, a.nquartet);
+  int ibw = -1, tb_bra = -1;  // running bra; bra whose product table Tb holds
+  for (int64_t q = qbeg; q < qend; ++q) {
+    int ib = 0;
+    if (lane == 0) {
+      if (ibw < 0) {
+        ibw = find_bra(a.qoff, a.nbra, q);
+      } else {
+        int steps = 0;
+        while (q >= a.qoff[ibw + 1] && steps < 32) {
+          ++ibw;
+          ++steps;
+        }
+        if (q >= a.qoff[ibw + 1]) ibw = find_bra(a.qoff, a.nbra, q);
+      }
+      ib = ibw;
+    }
+    ib = __shfl_sync(0xffffffffu, ib, 0);
+    ibw = ib;
+    const int ic = (int)(q - a.qoff[ib]) + (a.kbase ? a.kbase[ib] : 0);
+    const PairRec br = load_pair_fock(a.bra + ib), kt = load_pair_fock(a.ket + ic);
+    const int sel = quartet_select(a, br, kt, a.bra + ib, a.ket + ic);
+    if (sel) {
+      if (lane == 0 && sel == 2 && a.mode != 2) ++cnt_s;
+      continue;
+    }
+    double w = 1.0;
+    if (br.same) w *= 0.5;
+    if (kt.same) w *= 0.5;
+    if (a.same_class && ib == ic + a.ket_off) w *= 0.5;
+    // Single primitive pair on each side (the host launches this kernel only for such classes).
+    {
+      const PrimPair P1 = load_prim<true>(a.pp + br.pp0);
+      __syncwarp();
+      if (tb_bra != ib) {
+        if (lane < 3) {
+          const double pa = lane == 0 ? P1.PAx : lane == 1 ? P1.PAy : P1.PAz;
+          const double pb = lane == 0 ? P1.PBx : lane == 1 ? P1.PBy : P1.PBz;
+          herm_e<LA, LB, 1, Tc>(Tc(0.5 / P1.p), Tc(pa), Tc(pb), Eb + lane * EA);
+        }
+        __syncwarp();
+        wq_product_table<LA, LB, Tc>(Eb, Tb, lane);
+        tb_bra = ib;
+      }
+      {
+        const PrimPair P2 = load_prim<true>(a.pp + (a.ket_pp0 >= 0 ? a.ket_pp0 + ic : kt.pp0));
+        __syncwarp();
+        if (lane < 3) {
+          const double pa = lane == 0 ? P2.PAx : lane == 1 ? P2.PAy : P2.PAz;
+          const double pb = lane == 0 ? P2.PBx : lane == 1 ? P2.PBy : P2.PBz;
+          herm_e<LC, LD, -1, Tc>(Tc(0.5 / P2.p), Tc(pa), Tc(pb), Ek + lane * EC);
+        }
+        // Boys function and scaled R^n_000 (every lane, the same values)
+        const double rs = (sizeof(Tc) == 4) ? (double)rsqrtf((float)(P1.p + P2.p)) : rsqrt(P1.p + P2.p);
+        const double alpha = P1.p * P2.p * rs * rs;
+        const double x = P1.Px - P2.Px, y = P1.Py - P2.Py, z = P1.Pz - P2.Pz;
+        double F[L + 1];
+        boys_eval<L, (sizeof(Tc) == 4) ? kBoysDegLow : kBoysDeg>(alpha * (x * x + y * y + z * z), tab, F);
+        double Fs[L + 1];
+        {
+          double s = P1.K * P2.K * rs;
+#pragma unroll
+          for (int n = 0; n <= L; ++n) {
+            Fs[n] = s * F[n];
+            s *= -2.0 * alpha;
+          }
+        }
+        __syncwarp();
+        wq_product_table<LC, LD, Tc>(Ek, Tk, lane);
+        // R_tuv, level n = L-1 .. 0 from level n+1, ping-pong between R0 and R1
+        Tc *prev = R0, *cur = R1;
+        if (lane == 0) prev[0] = Tc(Fs[L]);
+        __syncwarp();
+        const Tc tx = Tc(x), ty = Tc(y), tz = Tc(z);
+#pragma unroll 1
+        for (int n = L - 1; n >= 0; --n) {
+          const int cnt = n3(L - n);
+          for (int e = lane; e < cnt; e += 32) {
+            const int pos = tuvt[e];
+            const int t = pos / (BOX * BOX), u = (pos / BOX) % BOX, v = pos % BOX;
+            Tc val;
+            if (e == 0) {
+              val = Tc(Fs[n]);
+            } else if (t > 0) {
+              val = tx * prev[pos - BOX * BOX];
+              if (t > 1) val += Tc(t - 1) * prev[pos - 2 * BOX * BOX];
+            } else if (u > 0) {
+              val = ty * prev[pos - BOX];
+              if (u > 1) val += Tc(u - 1) * prev[pos - 2 * BOX];
+            } else {
+              val = tz * prev[pos - 1];
+              if (v > 1) val += Tc(v - 1) * prev[pos - 2];
+            }
+            cur[pos] = val;
+          }
+          __syncwarp();
+          Tc *sw = prev;
+          prev = cur;
+          cur = sw;
+        }
+        const Tc *R = prev;
+        // ket transform: lane = bra Hermite index, every ket component
+        for (int e = lane; e < N3AB; e += 32) {
+          const int base = tuvt[e];
+          Tc xa[NCD];
+#pragma unroll
+          for (int cd = 0; cd < NCD; ++cd) xa[cd] = Tc(0);
+          wq::static_for<N3CD>([&](auto F_) {
+            constexpr int f = decltype(F_)::value;
+            constexpr int ft = wq::tuv_t(f), fu = wq::tuv_u(f), fv = wq::tuv_v(f);
+            const Tc r = R[base + (ft * BOX + fu) * BOX + fv];
+            wq::static_for<NCD>([&](auto CD_) {
+              constexpr int cd = decltype(CD_)::value;
+              if constexpr (wq::uses(LC, LD, cd, ft, fu, fv)) xa[cd] += Tk[wq::term_at(LC, LD, cd, ft, fu, fv)] * r;
+            });
+          });
+#pragma unroll
+          for (int cd = 0; cd < NCD; ++cd) X[cd * PX + e] = xa[cd];
+        }
+        __syncwarp();
+      }
+      // bra transform: lane = ket component, every bra component
+      for (int cd = lane; cd < NCD; cd += 32) {
+        Tc acc[NAB];
+#pragma unroll
+        for (int ab = 0; ab < NAB; ++ab) acc[ab] = Tc(0);
+        wq::static_for<N3AB>([&](auto E_) {
+          constexpr int e = decltype(E_)::value;
+          constexpr int et = wq::tuv_t(e), eu = wq::tuv_u(e), ev = wq::tuv_v(e);
+          const Tc xv = X[cd * PX + e];
+          wq::static_for<NAB>([&](auto AB_) {
+            constexpr int ab = decltype(AB_)::value;
+            if constexpr (wq::uses(LA, LB, ab, et, eu, ev)) acc[ab] += Tb[wq::term_at(LA, LB, ab, et, eu, ev)] * xv;
+          });
+        });
+#pragma unroll
+        for (int ab = 0; ab < NAB; ++ab) Gc[ab * PG + cd] = (double)acc[ab];
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      cnt_q += 1;
+      cnt_p += 1;
+    }
+    if (a.spherical)
+      wq_finish<LA, LB, LC, LD, Tc, true>(a, Gc, Gs, Gf, Db, sph, br, kt, ib, ic, w, lane);
+    else
+      wq_finish<LA, LB, LC, LD, Tc, false>(a, Gc, Gs, Gf, Db, sph, br, kt, ib, ic, w, lane);
+    __syncwarp();
+  }
+  if (lane == 0 && a.counters) {
+    atomicAdd(a.counters + 0, cnt_q);
+    atomicAdd(a.counters + 1, cnt_p);
+    atomicAdd(a.counters + 2, cnt_s);
+    if (sizeof(Tc) == 4) atomicAdd(a.counters + 3, cnt_q);
+  }
+}
+
+}  // namespace dgf

@@ -141,6 +141,13 @@ __device__ __forceinline__ PairRec load_pair_fock(const PairRec *p) {
   return r;
 }
 
+// Dalton blocks of a pair's shells: {block A, block B, A whole, B whole}.
+__device__ __forceinline__ int4 block_of_pair(const PairRec *p) {
+  const int4 v = __ldg(reinterpret_cast<const int4 *>(p) + 3);  // atA, atB, blkA, blkB
+  return make_int4(v.z & (kWholeBlock - 1), v.w & (kWholeBlock - 1), (v.z & kWholeBlock) ? 1 : 0,
+                   (v.w & kWholeBlock) ? 1 : 0);
+}
+
 template <bool PAB>
 __device__ __forceinline__ PrimPair load_prim(const PrimPair *p) {
   PrimPair r;

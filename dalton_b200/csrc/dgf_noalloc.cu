@@ -48,7 +48,10 @@ std::mutex g_setup_mutex;
 
 // Device address of the scratch array on the current device, looked up once
 // per device by the first call made on it (make that call before any stream
-// capture).
+// capture).  The address stays valid for the life of the device's primary
+// context: after a cudaDeviceReset on that device the cached address is
+// stale, so a process that resets a device must not call this entry point
+// on it again.
 cudaError_t scratch_address(int device, double **out) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (!g_scratch_addr[device]) {
@@ -127,8 +130,11 @@ extern "C" int dgf_fock_device_noalloc(dgf_ctx *c, const double *dmat_device, do
     const int lc = (cp.Y == 0) ? 0 : (cp.Y <= 2) ? 1 : (cp.Y <= 5) ? 2 : 3;
     const int ld = cp.Y - lc * (lc + 1) / 2;
     a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-    const ClassKernel *k = &jk_kernel_variant(cp.X, cp.Y, 0, c->choice[cp.X][cp.Y][0], cp.bucket == 0);
-    if (!k->launch) k = &jk_kernel(cp.X, cp.Y, 0, cp.bucket == 0);
+    if (cp.nquartet <= 0) continue;
+    const bool bra1 = c->cls_max_npp[cp.X] == 1;
+    const ClassKernel *k = &jk_kernel_variant(cp.X, cp.Y, 0, c->choice[cp.X][cp.Y][0], cp.bucket == 0, bra1);
+    if (!k->launch) k = &jk_kernel(cp.X, cp.Y, 0, cp.bucket == 0, bra1);
+    if (!k->launch) return fail(DGF_ERR_UNSUPPORTED, __LINE__, "no kernel for this quartet class");
     const int64_t per_block = k->qpb;
     const int grid =
         (int)std::max<int64_t>(1, std::min<int64_t>((cp.nquartet + per_block - 1) / per_block, (int64_t)c->nsm * 16));

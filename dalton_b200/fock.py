@@ -82,8 +82,11 @@ class FockBuilder:
     def _ifctyp(ifctyp, nd):
         return np.ascontiguousarray(np.broadcast_to(np.asarray(ifctyp, dtype=np.int64), (nd,)))
 
-    def herfck(self, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, mixed_cutoff=0.0, shard=(0, 1)) -> np.ndarray:
-        """F = [Y&1] J[D] - [Y&2] hfxfac/2 K[D] for host matrices (N,N) or (ndmat,N,N)."""
+    def herfck(self, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, mixed_cutoff=0.0, shard=(0, 1),
+               icedif=3) -> np.ndarray:
+        """F = [Y&1] J[D] - [Y&2] hfxfac/2 K[D] for host matrices (N,N) or (ndmat,N,N).
+        Density screening (Dalton's .IFTHRS) is on for ifthrs < 16, with
+        Dalton's separate Coulomb/exchange skips per ``icedif`` (.ICEDIF)."""
         d = np.ascontiguousarray(dmat, dtype=np.float64)
         single = d.ndim == 2
         if single:
@@ -95,7 +98,7 @@ class FockBuilder:
         f = np.empty_like(d)
         opt = _lib.default_options(thrs=float(thrs), ifthrs=int(ifthrs), hfxfac=float(hfxfac),
                                    mixed_cutoff=float(mixed_cutoff), shard_index=int(shard[0]),
-                                   shard_count=int(shard[1]))
+                                   shard_count=int(shard[1]), icedif=int(icedif))
         st = _lib.DgfStats()
         _lib.check(self._lib.dgf_fock(self._h, nd, ift.ctypes.data_as(ctypes.POINTER(_lib.dgf_int)), _dp(d), _dp(f),
                                       ctypes.byref(opt), ctypes.byref(st)), "dgf_fock")
@@ -103,7 +106,7 @@ class FockBuilder:
         return f[0] if single else f
 
     def herfck_device(self, dmat, fmat=None, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, mixed_cutoff=0.0,
-                      stream=None, stats=True, shard=(0, 1)):
+                      stream=None, stats=True, shard=(0, 1), icedif=3):
         """Device form: ``dmat`` a CUDA float64 tensor (N,N) or (ndmat,N,N)."""
         import torch
 
@@ -116,7 +119,7 @@ class FockBuilder:
         ift = self._ifctyp(ifctyp, nd)
         opt = _lib.default_options(thrs=float(thrs), ifthrs=int(ifthrs), hfxfac=float(hfxfac),
                                    mixed_cutoff=float(mixed_cutoff), shard_index=int(shard[0]),
-                                   shard_count=int(shard[1]))
+                                   shard_count=int(shard[1]), icedif=int(icedif))
         if stream is None:
             stream = torch.cuda.current_stream(d.device).cuda_stream
         st = _lib.DgfStats()

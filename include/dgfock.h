@@ -16,7 +16,7 @@
  *       J_pq = sum_rs (pq|rs) D_rs,   K_pq = sum_rs (pr|qs) D_rs
  *     (FCKD03, sirfck.F:1496-1547; FCKCON, herfckcon.F:20-220).
  *   - Shell quartets with Q_AB*Q_CD < thrs are skipped (Schwarz, THRS
- *     default 1e-12, herrdn.F:359; her2gab.F GABGEN); with ifthrs < 20 also
+ *     default 1e-12, herrdn.F:359; her2gab.F GABGEN); with ifthrs < 16 also
  *     those with Q_AB*Q_CD*max(4|D|_Coulomb, |D|_exchange) < 10^-ifthrs
  *     (SYMLOP screening, her2drv.F:2663-2733).
  *   - Errors are returned as status codes (0 = success), never by aborting;
@@ -87,7 +87,9 @@ typedef struct {
 
 /* Fock-build options (no globals; Dalton's COMMON values passed in).
  * thrs: Schwarz threshold (THRS, 1e-12 default);
- * ifthrs: density screening exponent (>= 20 disables, HR2INP .IFTHRS);
+ * ifthrs: density screening exponent (HR2INP .IFTHRS): on when ifthrs < 16
+ *   as in Dalton's direct Fock build (values below 4 are taken as 14,
+ *   DALTON/abacus/her2drv.F:520-540);
  * hfxfac: exchange factor (HFXFAC, 1 for HF);
  * mixed_cutoff: 0 = all-FP64 drop-in; > 0 = quartets whose bound
  *   Q_AB*Q_CD*Dmax is below it are evaluated in FP32 (Boys function,
@@ -97,16 +99,27 @@ typedef struct {
   dgf_int ifthrs;
   double hfxfac;
   double mixed_cutoff;
-  /* Shard of the quartet queue this call evaluates: every class's canonical
-   * quartet list is cut into shard_count equal contiguous ranges and range
-   * shard_index is evaluated, so each shard does 1/shard_count of every
-   * class; F is then the partial sum of that shard (sum the shards, e.g.
-   * with an NCCL all-reduce, for the full matrix).  0 and 1 = everything. */
+  /* Shard of the quartet queue this call evaluates: the class-sorted queue
+   * (all classes in order) is cut into shard_count contiguous ranges of equal
+   * model cost (a fixed FLOP model per class, the same on every rank) and
+   * range shard_index is evaluated, as Dalton's parallel Fock build hands
+   * cost-sorted shell-pair tasks to its workers (herpar.F:457,1165); F is
+   * then the partial sum of that shard (sum the shards, e.g. with an NCCL
+   * all-reduce, for the full matrix).  0 and 1 = everything. */
   dgf_int shard_index;
   dgf_int shard_count;
+  /* ICEDIF (HR2INP .ICEDIF, DALTON/abacus/herdrv.F:2042-2044,2131): with
+   * density screening on, bit 1 drops a quartet's Coulomb contribution of a
+   * density when max|D| over its Coulomb blocks times the quartet's largest
+   * integral is below 10^-ifthrs, bit 2 likewise its exchange contribution
+   * (INTFC1, DALTON/abacus/her2fck.F:221-222,446-466).  Dalton's default is
+   * 3.  The thread-per-quartet kernels apply it; quartets of the cooperative
+   * kernels are always digested whole (the conservative side). */
+  dgf_int icedif;
 } dgf_options;
 
-/* Default options: thrs 1e-12, ifthrs 20, hfxfac 1, mixed_cutoff 0, one shard. */
+/* Default options: thrs 1e-12, ifthrs 20, hfxfac 1, mixed_cutoff 0, one
+ * shard, icedif 3. */
 void dgf_default_options(dgf_options *opt);
 
 /* Create a context on CUDA device `device`: copies the basis to the device,
@@ -133,7 +146,7 @@ int dgf_fock_device(dgf_ctx *ctx, dgf_int ndmat, const dgf_int *ifctyp, const do
  * Fock matrix, such as a host that, like Dalton, gives the engine one fixed
  * work area and nothing more, or a process whose device memory is owned by
  * another pool.  Same result as dgf_fock_device with ndmat = 1, IFCTYP 13,
- * ifthrs >= 20, mixed_cutoff = 0: F = J[D] - hfxfac/2 K[D] of one density
+ * ifthrs >= 16, mixed_cutoff = 0: F = J[D] - hfxfac/2 K[D] of one density
  * (symmetrised), device pointers.  Its scratch is a fixed device array of
  * 3 x 1536 x 1536 doubles (56.6 MB: density, D + D^T and half Fock matrix of
  * the two-electron working basis, in which general contractions are resolved
@@ -143,7 +156,8 @@ int dgf_fock_device(dgf_ctx *ctx, dgf_int ndmat, const dgf_int *ifctyp, const do
  * (an earlier dgf_fock, dgf_fock_device, dgf_autotune or dgf_grad2e call
  * with this threshold builds it), else DGF_ERR_ARG.  The first call on a
  * device looks up the array's device address; make it before any CUDA
- * stream capture.  All calls share the array and leave its contents behind;
+ * stream capture.  The address is kept for the life of the device's
+ * context: after a cudaDeviceReset of that device do not call it again.  All calls share the array and leave its contents behind;
  * calls that overlap on the GPU (other streams or host threads) race and
  * must be serialised by the caller. */
 int dgf_fock_device_noalloc(dgf_ctx *ctx, const double *dmat_device, double *fmat_device, double hfxfac,
@@ -183,7 +197,9 @@ int dgf_grad1e(dgf_ctx *ctx, const double *dmat, const double *wmat, double *gra
 typedef struct {
   int32_t la, lb, lc, ld;   /* angular momenta of the class (ab|cd) */
   int32_t precision;        /* 64 = FP64, 32 = FP32 contraction */
-  int32_t kernel;           /* 0 = thread-per-quartet, 1 = cooperative team, 2 = warp teams */
+  int32_t kernel;           /* 0 = thread-per-quartet, 1 = cooperative team, 2 = warp teams,
+                               3 = thread-per-quartet reading the bra's density rows from shared
+                               memory, 4 = warp-per-quartet (single primitive pairs, L >= 6) */
   int64_t quartets;         /* quartets of the class in the plan */
   int64_t evaluated;        /* quartets this launch evaluated */
   int64_t prim_quartets;    /* primitive quartets this launch evaluated */

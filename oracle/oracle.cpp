@@ -24,11 +24,16 @@ inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
 // Dalton Cartesian order: x-exponent descending, then y descending
 // (xx, xy, xz, yy, yz, zz) — DALTON/abacus/hergam.F:164-218.
-std::vector<std::array<int, 3>> cart_list(int l) {
-  std::vector<std::array<int, 3>> v;
-  for (int i = l; i >= 0; --i)
-    for (int j = l - i; j >= 0; --j) v.push_back({i, j, l - i - j});
-  return v;
+// Tables are built once (l <= 8) and returned by reference.
+const std::vector<std::array<int, 3>> &cart_list(int l) {
+  static const std::vector<std::vector<std::array<int, 3>>> tab = [] {
+    std::vector<std::vector<std::array<int, 3>>> t(9);
+    for (int ll = 0; ll <= 8; ++ll)
+      for (int i = ll; i >= 0; --i)
+        for (int j = ll - i; j >= 0; --j) t[ll].push_back({i, j, ll - i - j});
+    return t;
+  }();
+  return tab[l];
 }
 
 double binom(int n, int k) {
@@ -190,6 +195,7 @@ void hermite_r(int L, double alpha, double x, double y, double z, RWork &w, std:
 
 struct Shell {
   int l, atom, nprim, ao, nf;
+  int blk;  // Dalton block (atom, l, general contraction) the shell comes from
   double xyz[3];
   std::vector<double> a, c;
 };
@@ -197,6 +203,7 @@ struct Shell {
 struct Basis {
   int nbf, natom, spherical, maxl;
   std::vector<Shell> sh;
+  std::vector<int> blk_ao0, blk_nfun;  // per Dalton block: first AO function, number of functions
   std::vector<double> xyz, charge;
   std::vector<std::vector<double>> sph;  // per l: nf x ncart
 };
@@ -216,9 +223,12 @@ Basis make_basis(const orc_basis *b) {
     int np = (int)b->block_nprim[ib], nc = (int)b->block_ncontr[ib];
     int nf = (B.spherical && l >= 2) ? 2 * l + 1 : ncart(l);
     B.maxl = std::max(B.maxl, l);
+    B.blk_ao0.push_back((int)b->block_ao_offset[ib]);
+    B.blk_nfun.push_back(nc * nf);
     for (int k = 0; k < nc; ++k) {
       Shell s;
       s.l = l;
+      s.blk = ib;
       s.atom = (int)b->block_atom[ib];
       s.ao = (int)b->block_ao_offset[ib] + k * nf;
       s.nf = nf;
@@ -279,7 +289,7 @@ void prim_eri(int la, int lb, int lc, int ld, double a, double b, double c, doub
   int L = la + lb + lc + ld, n1 = L + 1;
   hermite_r(L, alpha, P[0] - Q[0], P[1] - Q[1], P[2] - Q[2], w.rw, w.R);
   int Lab = la + lb, Lcd = lc + ld;
-  auto ca = cart_list(la), cb = cart_list(lb), cc = cart_list(lc), cd = cart_list(ld);
+  const auto &ca = cart_list(la), &cb = cart_list(lb), &cc = cart_list(lc), &cd = cart_list(ld);
   int nab1 = Lab + 1, ncd1 = Lcd + 1;
   size_t box = (size_t)nab1 * nab1 * nab1;
   int ncc = (int)cc.size(), ncdd = (int)cd.size();
@@ -470,113 +480,419 @@ int orc_eri_full(const orc_basis *b, double *eri) {
 // HERFCK semantics through FCKD03-style digestion of unique integrals
 // (DALTON/sirius/sirfck.F:1496-1547; IFCTYP decoding sirfck.F:45-57 and
 // DALTON/abacus/herfckcon.F:20-220).
+//
+// Density screening restates Dalton's direct-Fock screening, which is on
+// when IFTHRS < 16 (DALTON/abacus/her2drv.F:520-540; IFTHRS < 4 is reset to
+// 14 there):
+//  * SYMLOP (her2drv.F:2663-2733): per Dalton block quartet, with GAB the
+//    block Schwarz factors and DMRAO the block maxima of |D| per density,
+//    DNSBUF(1) = max |D| over the AB, BA, CD, DC blocks (Coulomb),
+//    DNSBUF(2) = max over the CA, AC, CB, BC, DA, AD, BD, DB blocks
+//    (exchange, 0 when HFXFAC = 0), DNSMAX = max over densities of
+//    max(4 DNSBUF(1), DNSBUF(2)); the quartet is skipped when
+//    GAB_AB GAB_CD DNSMAX < 10^-IFTHRS.
+//  * INTFCK/INTFC1 (DALTON/abacus/her2fck.F:84-90, 221-222, 446-466):
+//    integrals with |g| <= max(10^-IFTHRS / DNSMAX, 1e-15) are dropped; with
+//    AOMAX the largest kept |g|, density I's Coulomb part is skipped when
+//    bit 1 of ICEDIF is set and DNSBUF(1,I) AOMAX < 10^-IFTHRS, its exchange
+//    part when bit 2 is set and DNSBUF(2,I) AOMAX < 10^-IFTHRS.
+// The block quantities use Dalton's blocks (one atom's shell of angular
+// momentum l with all its contracted functions); AOMAX is taken per
+// segmented shell quartet, the unit this restatement evaluates.  Whatever
+// IFTHRS is, quartets whose density bound is exactly zero contribute nothing
+// and are skipped without evaluation.
+struct FockOpts {
+  double hfxfac = 1.0, thrs = 1e-12;
+  int ifthrs = 20, icedif = 3;
+  int stride = 1, offset = 0;
+};
+
+struct FockCounts {
+  int64_t evaluated = 0, skipped_screen = 0, skipped_zero = 0, dropped_j = 0, dropped_k = 0;
+};
+
+// Block Schwarz factors and block density maxima.
+struct BlockBounds {
+  int nb = 0;
+  std::vector<double> gab;    // nb x nb
+  std::vector<double> dmax;   // ndmat x nb x nb, max |D_pq| over p in block A, q in block B
+};
+
+static BlockBounds block_bounds(const Basis &B, const std::vector<double> &Q, const double *D, int ndmat) {
+  BlockBounds bb;
+  bb.nb = (int)B.blk_ao0.size();
+  const int nb = bb.nb, ns = (int)B.sh.size();
+  const size_t N = B.nbf;
+  bb.gab.assign((size_t)nb * nb, 0.0);
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b < ns; ++b) {
+      double &g = bb.gab[(size_t)B.sh[a].blk * nb + B.sh[b].blk];
+      g = std::max(g, Q[(size_t)a * ns + b]);
+    }
+  bb.dmax.assign((size_t)ndmat * nb * nb, 0.0);
+  for (int k = 0; k < ndmat; ++k)
+    for (int A = 0; A < nb; ++A)
+      for (int Bk = 0; Bk < nb; ++Bk) {
+        double m = 0.0;
+        for (int p = B.blk_ao0[A]; p < B.blk_ao0[A] + B.blk_nfun[A]; ++p)
+          for (int q = B.blk_ao0[Bk]; q < B.blk_ao0[Bk] + B.blk_nfun[Bk]; ++q)
+            m = std::max(m, std::fabs(D[k * N * N + p * N + q]));
+        bb.dmax[((size_t)k * nb + A) * nb + Bk] = m;
+      }
+  return bb;
+}
+
 static int fock_core(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
-                     double hfxfac, double thrs, int stride, int offset, int64_t *nquartet);
+                     const FockOpts &o, FockCounts *counts);
 
 int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
              double hfxfac, double thrs) {
-  return fock_core(b, ndmat, ifctyp, dmat, fmat, hfxfac, thrs, 1, 0, nullptr);
+  FockOpts o;
+  o.hfxfac = hfxfac;
+  o.thrs = thrs;
+  return fock_core(b, ndmat, ifctyp, dmat, fmat, o, nullptr);
+}
+
+int orc_fock_screened(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
+                      double hfxfac, double thrs, int64_t ifthrs, int64_t icedif, int64_t *counts) {
+  FockOpts o;
+  o.hfxfac = hfxfac;
+  o.thrs = thrs;
+  o.ifthrs = (int)ifthrs;
+  o.icedif = (int)icedif;
+  FockCounts c;
+  int r = fock_core(b, ndmat, ifctyp, dmat, fmat, o, &c);
+  if (counts) {
+    counts[0] = c.evaluated;
+    counts[1] = c.skipped_screen;
+    counts[2] = c.skipped_zero;
+    counts[3] = c.dropped_j;
+    counts[4] = c.dropped_k;
+  }
+  return r;
 }
 
 int orc_fock_sampled(const orc_basis *b, const double *dmat, double *fmat, double thrs, int stride, int offset,
                      int64_t *nquartet) {
   const int64_t ift = 13;
-  return fock_core(b, 1, &ift, dmat, fmat, 1.0, thrs, stride, offset, nquartet);
+  FockOpts o;
+  o.thrs = thrs;
+  o.stride = stride;
+  o.offset = offset;
+  FockCounts c;
+  int r = fock_core(b, 1, &ift, dmat, fmat, o, &c);
+  if (nquartet) *nquartet = c.evaluated;
+  return r;
 }
 
-static int fock_core(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
-                     double hfxfac, double thrs, int stride, int offset, int64_t *nquartet) {
-  set_threads();
-  Basis B = make_basis(b);
-  int ns = (int)B.sh.size();
-  size_t N = B.nbf, N2 = N * N;
-  std::vector<double> D(ndmat * N2);
-  std::vector<int> doJ(ndmat), doK(ndmat);
+// Decoded IFCTYP of each density: symmetrised / antisymmetrised / general D,
+// and whether it takes Coulomb and exchange parts.
+struct DensitySet {
+  std::vector<double> D;
+  std::vector<int> doJ, doK;
+};
+
+static DensitySet decode_densities(size_t N, int ndmat, const int64_t *ifctyp, const double *dmat, double hfxfac) {
+  DensitySet ds;
+  const size_t N2 = N * N;
+  ds.D.assign(ndmat * N2, 0.0);
+  ds.doJ.assign(ndmat, 0);
+  ds.doK.assign(ndmat, 0);
   for (int k = 0; k < ndmat; ++k) {
     int X = (int)(ifctyp[k] / 10), Y = (int)(ifctyp[k] % 10);
     if (X == 2) Y &= 2;
     if (hfxfac == 0.0) Y &= 1;
-    doJ[k] = Y & 1;
-    doK[k] = (Y & 2) ? 1 : 0;
+    ds.doJ[k] = Y & 1;
+    ds.doK[k] = (Y & 2) ? 1 : 0;
     for (size_t p = 0; p < N; ++p)
       for (size_t q = 0; q < N; ++q) {
         double dpq = dmat[k * N2 + p * N + q], dqp = dmat[k * N2 + q * N + p];
-        D[k * N2 + p * N + q] = (X == 1) ? 0.5 * (dpq + dqp) : (X == 2) ? 0.5 * (dpq - dqp) : dpq;
+        ds.D[k * N2 + p * N + q] = (X == 1) ? 0.5 * (dpq + dqp) : (X == 2) ? 0.5 * (dpq - dqp) : dpq;
       }
   }
+  return ds;
+}
+
+// Digestion of one segmented shell quartet block g (FCKCON, herfckcon.F:66-80,
+// in the FCKD03 form that handles general densities), with Dalton's
+// per-density Coulomb/exchange skips; Fl accumulates (ndmat x N x N).
+static void digest_quartet(const Basis &B, int sA, int sB, int sC, int sD, bool same_pair, const std::vector<double> &g,
+                           const DensitySet &ds, int ndmat, double efac, const double *jkeep, const double *kkeep,
+                           double fcktol, double *Fl) {
+  const size_t N = B.nbf, N2 = N * N;
+  const Shell &A = B.sh[sA], &Bs = B.sh[sB], &C = B.sh[sC], &Dd = B.sh[sD];
+  for (int i = 0; i < A.nf; ++i) {
+    size_t p = A.ao + i;
+    for (int j = 0; j < Bs.nf; ++j) {
+      size_t q = Bs.ao + j;
+      if (sA == sB && q > p) continue;
+      for (int kk = 0; kk < C.nf; ++kk) {
+        size_t r = C.ao + kk;
+        for (int m = 0; m < Dd.nf; ++m) {
+          size_t s = Dd.ao + m;
+          if (sC == sD && s > r) continue;
+          if (same_pair && (r * (r + 1) / 2 + s) > (p * (p + 1) / 2 + q)) continue;
+          double gint = g[((i * Bs.nf + j) * C.nf + kk) * Dd.nf + m];
+          if (std::fabs(gint) <= fcktol) continue;
+          if (p == q) gint *= 0.5;
+          if (r == s) gint *= 0.5;
+          if (p == r && q == s) gint *= 0.5;
+          for (int k = 0; k < ndmat; ++k) {
+            const double *Dk = &ds.D[k * N2];
+            double *Fk = &Fl[k * N2];
+            if (ds.doJ[k] && jkeep[k] != 0.0) {
+              double fadd = gint * (Dk[r * N + s] + Dk[s * N + r]);
+              Fk[p * N + q] += fadd;
+              Fk[q * N + p] += fadd;
+              fadd = gint * (Dk[p * N + q] + Dk[q * N + p]);
+              Fk[r * N + s] += fadd;
+              Fk[s * N + r] += fadd;
+            }
+            if (ds.doK[k] && kkeep[k] != 0.0) {
+              double e = efac * gint;
+              Fk[p * N + r] -= e * Dk[q * N + s];
+              Fk[r * N + p] -= e * Dk[s * N + q];
+              Fk[p * N + s] -= e * Dk[q * N + r];
+              Fk[s * N + p] -= e * Dk[r * N + q];
+              Fk[q * N + r] -= e * Dk[p * N + s];
+              Fk[r * N + q] -= e * Dk[s * N + p];
+              Fk[q * N + s] -= e * Dk[p * N + r];
+              Fk[s * N + q] -= e * Dk[r * N + p];
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// Screening decision of one segmented quartet (SYMLOP on its Dalton
+// blocks): returns 0 = evaluate, 1 = screened out, 2 = zero density bound;
+// dJ/dK receive DNSBUF(1/2, I), *dnsmax DNSMAX.
+static int quartet_screen(const Basis &B, const BlockBounds &bb, int sA, int sB, int sC, int sD, int ndmat,
+                          double hfxfac, bool doscrn, double fckthr, double *dJ, double *dK, double *dnsmax) {
+  const int nb = bb.nb;
+  const int a = B.sh[sA].blk, b = B.sh[sB].blk, c = B.sh[sC].blk, d = B.sh[sD].blk;
+  double dm = 0.0;
+  for (int k = 0; k < ndmat; ++k) {
+    const double *M = &bb.dmax[(size_t)k * nb * nb];
+    auto at = [&](int x, int y) { return M[(size_t)x * nb + y]; };
+    dJ[k] = std::max(std::max(at(a, b), at(b, a)), std::max(at(c, d), at(d, c)));
+    dK[k] = 0.0;
+    if (hfxfac != 0.0)
+      dK[k] = std::max(std::max(std::max(at(c, a), at(a, c)), std::max(at(c, b), at(b, c))),
+                       std::max(std::max(at(d, a), at(a, d)), std::max(at(b, d), at(d, b))));
+    dm = std::max(dm, std::max(4.0 * dJ[k], dK[k]));
+  }
+  *dnsmax = dm;
+  if (dm == 0.0) return 2;
+  if (doscrn && dm * bb.gab[(size_t)a * nb + b] * bb.gab[(size_t)c * nb + d] < fckthr) return 1;
+  return 0;
+}
+
+static int fock_core(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
+                     const FockOpts &o, FockCounts *counts) {
+  set_threads();
+  Basis B = make_basis(b);
+  int ns = (int)B.sh.size();
+  size_t N = B.nbf, N2 = N * N;
+  const DensitySet ds = decode_densities(N, ndmat, ifctyp, dmat, o.hfxfac);
   std::vector<double> Q = schwarz(B);
+  const BlockBounds bb = block_bounds(B, Q, ds.D.data(), ndmat);
+  int ifthrs = o.ifthrs;
+  if (ifthrs < 4) ifthrs = 14;
+  const bool doscrn = ifthrs < 16;
+  const double fckthr = std::pow(10.0, -(double)ifthrs);
   std::vector<std::pair<int, int>> pairs;
   for (int a = 0; a < ns; ++a)
-    for (int bb = 0; bb <= a; ++bb) pairs.push_back({a, bb});
+    for (int bb2 = 0; bb2 <= a; ++bb2) pairs.push_back({a, bb2});
   int npair = (int)pairs.size();
   std::vector<double> F(ndmat * N2, 0.0);
-  double efac = 0.5 * hfxfac;
-  int64_t nq_total = 0;
-#pragma omp parallel reduction(+ : nq_total)
+  double efac = 0.5 * o.hfxfac;
+  int64_t nq = 0, nscr = 0, nzero = 0, ndj = 0, ndk = 0;
+#pragma omp parallel reduction(+ : nq, nscr, nzero, ndj, ndk)
   {
     std::vector<double> Fl(ndmat * N2, 0.0);
+    std::vector<double> dJ(ndmat), dK(ndmat), jkeep(ndmat), kkeep(ndmat);
     EriWork w;
     std::vector<double> g, cart, tmp;
 #pragma omp for schedule(dynamic)
     for (int ab = npair - 1; ab >= 0; --ab) {
-      if (ab % stride != offset) continue;
+      if (ab % o.stride != o.offset) continue;
       int sA = pairs[ab].first, sB = pairs[ab].second;
       double qab = Q[(size_t)sA * ns + sB];
       for (int cd = 0; cd <= ab; ++cd) {
         int sC = pairs[cd].first, sD = pairs[cd].second;
-        if (qab * Q[(size_t)sC * ns + sD] < thrs) continue;
-        ++nq_total;
+        if (qab * Q[(size_t)sC * ns + sD] < o.thrs) continue;
+        double dnsmax = 0.0;
+        const int scr = quartet_screen(B, bb, sA, sB, sC, sD, ndmat, o.hfxfac, doscrn, fckthr, dJ.data(),
+                                       dK.data(), &dnsmax);
+        if (scr == 2) {
+          ++nzero;
+          continue;
+        }
+        if (scr == 1) {
+          ++nscr;
+          continue;
+        }
+        ++nq;
         shell_eri(B, sA, sB, sC, sD, g, w, cart, tmp);
-        const Shell &A = B.sh[sA], &Bs = B.sh[sB], &C = B.sh[sC], &Dd = B.sh[sD];
-        for (int i = 0; i < A.nf; ++i) {
-          size_t p = A.ao + i;
-          for (int j = 0; j < Bs.nf; ++j) {
-            size_t q = Bs.ao + j;
-            if (sA == sB && q > p) continue;
-            for (int kk = 0; kk < C.nf; ++kk) {
-              size_t r = C.ao + kk;
-              for (int m = 0; m < Dd.nf; ++m) {
-                size_t s = Dd.ao + m;
-                if (sC == sD && s > r) continue;
-                if (ab == cd && (r * (r + 1) / 2 + s) > (p * (p + 1) / 2 + q)) continue;
-                double gint = g[((i * Bs.nf + j) * C.nf + kk) * Dd.nf + m];
-                if (p == q) gint *= 0.5;
-                if (r == s) gint *= 0.5;
-                if (p == r && q == s) gint *= 0.5;
-                for (int k = 0; k < ndmat; ++k) {
-                  const double *Dk = &D[k * N2];
-                  double *Fk = &Fl[k * N2];
-                  if (doJ[k]) {
-                    double fadd = gint * (Dk[r * N + s] + Dk[s * N + r]);
-                    Fk[p * N + q] += fadd;
-                    Fk[q * N + p] += fadd;
-                    fadd = gint * (Dk[p * N + q] + Dk[q * N + p]);
-                    Fk[r * N + s] += fadd;
-                    Fk[s * N + r] += fadd;
-                  }
-                  if (doK[k]) {
-                    double e = efac * gint;
-                    Fk[p * N + r] -= e * Dk[q * N + s];
-                    Fk[r * N + p] -= e * Dk[s * N + q];
-                    Fk[p * N + s] -= e * Dk[q * N + r];
-                    Fk[s * N + p] -= e * Dk[r * N + q];
-                    Fk[q * N + r] -= e * Dk[p * N + s];
-                    Fk[r * N + q] -= e * Dk[s * N + p];
-                    Fk[q * N + s] -= e * Dk[p * N + r];
-                    Fk[s * N + q] -= e * Dk[r * N + p];
-                  }
-                }
-              }
+        double fcktol = -1.0;  // keep every integral unless screening is on
+        for (int k = 0; k < ndmat; ++k) jkeep[k] = kkeep[k] = 1.0;
+        if (doscrn) {
+          fcktol = std::max(fckthr / dnsmax, 1e-15);
+          double aomax = 0.0;
+          for (double v : g)
+            if (std::fabs(v) > fcktol) aomax = std::max(aomax, std::fabs(v));
+          for (int k = 0; k < ndmat; ++k) {
+            if ((o.icedif & 1) && ds.doJ[k] && dJ[k] * aomax < fckthr) {
+              jkeep[k] = 0.0;
+              ++ndj;
+            }
+            if ((o.icedif & 2) && ds.doK[k] && dK[k] * aomax < fckthr) {
+              kkeep[k] = 0.0;
+              ++ndk;
             }
           }
         }
+        digest_quartet(B, sA, sB, sC, sD, ab == cd, g, ds, ndmat, efac, jkeep.data(), kkeep.data(), fcktol,
+                       Fl.data());
       }
     }
 #pragma omp critical
     for (size_t i = 0; i < F.size(); ++i) F[i] += Fl[i];
   }
   std::memcpy(fmat, F.data(), F.size() * sizeof(double));
-  if (nquartet) *nquartet = nq_total;
+  if (counts) {
+    counts->evaluated = nq;
+    counts->skipped_screen = nscr;
+    counts->skipped_zero = nzero;
+    counts->dropped_j = ndj;
+    counts->dropped_k = ndk;
+  }
+  return 0;
+}
+
+// Class-stratified timing of the J+K build (IFCTYP 13, hfxfac 1, no density
+// screening) for the CPU baseline: the significant canonical quartets of the
+// segmented shells are counted per class (l_A l_B | l_C l_D); from each class
+// an evenly spaced sample is evaluated and digested (all threads), its
+// seconds per quartet are measured, and the full build's time is the sum
+// over classes of count x seconds per quartet.  Outputs per class (up to
+// maxcls): the four l values, the count, the sample size and the sample
+// seconds; *ncls = number of classes; *est_seconds = the extrapolated full
+// build, *total = all quartets.  target_seconds bounds the sampled work.
+int orc_fock_class_sample(const orc_basis *b, const double *dmat, double thrs, double target_seconds, int maxcls,
+                          int64_t *cls_l, int64_t *cls_count, int64_t *cls_sample, double *cls_seconds, int *ncls,
+                          double *est_seconds, int64_t *total) {
+  set_threads();
+  Basis B = make_basis(b);
+  const int ns = (int)B.sh.size();
+  const size_t N = B.nbf, N2 = N * N;
+  const int64_t ift = 13;
+  const DensitySet ds = decode_densities(N, 1, &ift, dmat, 1.0);
+  std::vector<double> Q = schwarz(B);
+  std::vector<std::pair<int, int>> pairs;
+  for (int a = 0; a < ns; ++a)
+    for (int c = 0; c <= a; ++c) pairs.push_back({a, c});
+  const int npair = (int)pairs.size();
+  const int L1 = B.maxl + 1;
+  auto key = [&](int a, int bq, int c, int d) {
+    return ((B.sh[a].l * L1 + B.sh[bq].l) * L1 + B.sh[c].l) * L1 + B.sh[d].l;
+  };
+  const int nkey = L1 * L1 * L1 * L1;
+  // counts per class
+  std::vector<int64_t> cnt(nkey, 0);
+#pragma omp parallel
+  {
+    std::vector<int64_t> cl(nkey, 0);
+#pragma omp for schedule(dynamic, 64)
+    for (int ab = 0; ab < npair; ++ab) {
+      const int sA = pairs[ab].first, sB = pairs[ab].second;
+      const double qab = Q[(size_t)sA * ns + sB];
+      for (int cd = 0; cd <= ab; ++cd) {
+        const int sC = pairs[cd].first, sD = pairs[cd].second;
+        if (qab * Q[(size_t)sC * ns + sD] >= thrs) ++cl[key(sA, sB, sC, sD)];
+      }
+    }
+#pragma omp critical
+    for (int k = 0; k < nkey; ++k) cnt[k] += cl[k];
+  }
+  // evenly spaced samples of at most smax quartets per class
+  auto collect = [&](const std::vector<int64_t> &want, std::vector<std::vector<std::pair<int, int>>> &out) {
+    out.assign(nkey, {});
+    std::vector<int64_t> stride(nkey, 1), seen(nkey, 0);
+    for (int k = 0; k < nkey; ++k) {
+      stride[k] = want[k] > 0 ? std::max<int64_t>(1, cnt[k] / want[k]) : 0;
+      if (want[k] > 0) out[k].reserve(want[k] + 1);
+    }
+    for (int ab = 0; ab < npair; ++ab) {
+      const int sA = pairs[ab].first, sB = pairs[ab].second;
+      const double qab = Q[(size_t)sA * ns + sB];
+      for (int cd = 0; cd <= ab; ++cd) {
+        const int sC = pairs[cd].first, sD = pairs[cd].second;
+        if (qab * Q[(size_t)sC * ns + sD] < thrs) continue;
+        const int k = key(sA, sB, sC, sD);
+        if (stride[k] && seen[k]++ % stride[k] == 0 && (int64_t)out[k].size() < want[k]) out[k].push_back({ab, cd});
+      }
+    }
+  };
+  auto run = [&](const std::vector<std::pair<int, int>> &smp) {
+    double t0 = omp_get_wtime();
+#pragma omp parallel
+    {
+      std::vector<double> Fl(N2, 0.0);
+      const double keep = 1.0;
+      EriWork w;
+      std::vector<double> g, cart, tmp;
+#pragma omp for schedule(dynamic, 4)
+      for (int64_t i = 0; i < (int64_t)smp.size(); ++i) {
+        const int ab = smp[i].first, cd = smp[i].second;
+        const int sA = pairs[ab].first, sB = pairs[ab].second, sC = pairs[cd].first, sD = pairs[cd].second;
+        shell_eri(B, sA, sB, sC, sD, g, w, cart, tmp);
+        digest_quartet(B, sA, sB, sC, sD, ab == cd, g, ds, 1, 0.5, &keep, &keep, -1.0, Fl.data());
+      }
+    }
+    return omp_get_wtime() - t0;
+  };
+  // calibration: a small sample per class gives seconds per quartet
+  int nclass = 0;
+  for (int k = 0; k < nkey; ++k) nclass += cnt[k] > 0;
+  std::vector<int64_t> want(nkey, 0);
+  for (int k = 0; k < nkey; ++k) want[k] = std::min<int64_t>(cnt[k], 256);
+  std::vector<std::vector<std::pair<int, int>>> smp;
+  collect(want, smp);
+  std::vector<double> spq(nkey, 0.0);
+  for (int k = 0; k < nkey; ++k)
+    if (!smp[k].empty()) spq[k] = run(smp[k]) / smp[k].size();
+  // main sample: each class gets an equal share of the time budget
+  const double share = target_seconds / std::max(nclass, 1);
+  for (int k = 0; k < nkey; ++k)
+    want[k] = cnt[k] ? std::min<int64_t>(cnt[k], std::max<int64_t>(256, (int64_t)(share / std::max(spq[k], 1e-9)))) : 0;
+  collect(want, smp);
+  double est = 0.0;
+  int64_t tot = 0;
+  int nout = 0;
+  for (int k = 0; k < nkey; ++k) {
+    if (!cnt[k]) continue;
+    const double sec = run(smp[k]);
+    est += sec / smp[k].size() * cnt[k];
+    tot += cnt[k];
+    if (nout < maxcls) {
+      int v = k;
+      for (int m = 3; m >= 0; --m) {
+        cls_l[4 * nout + m] = v % L1;
+        v /= L1;
+      }
+      cls_count[nout] = cnt[k];
+      cls_sample[nout] = (int64_t)smp[k].size();
+      cls_seconds[nout] = sec;
+    }
+    ++nout;
+  }
+  *ncls = nout;
+  *est_seconds = est;
+  *total = tot;
   return 0;
 }
 
@@ -644,8 +960,8 @@ int orc_grad2e(const orc_basis *b, const double *dmat, double hfxfac, double thr
                     prim_eri(lm[0], lm[1], lm[2], lm[3], ex[0], ex[1], ex[2], ex[3], S[0]->xyz, S[1]->xyz,
                              S[2]->xyz, S[3]->xyz, cc, cm.data(), w);
                 }
-          auto L0 = cart_list(l[0]), L1 = cart_list(l[1]), L2 = cart_list(l[2]), L3 = cart_list(l[3]);
-          std::vector<std::array<int, 3>> *Ls[4] = {&L0, &L1, &L2, &L3};
+          const std::vector<std::array<int, 3>> *Ls[4] = {&cart_list(l[0]), &cart_list(l[1]), &cart_list(l[2]),
+                                                          &cart_list(l[3])};
           int ncp[4], ncm[4];
           for (int i = 0; i < 4; ++i) {
             ncp[i] = ncart(lp[i]);
@@ -741,7 +1057,7 @@ void prim_one(const Basis &B, int kind, int la, int lb, double a, double b, cons
     ab2 += (A[i] - Bc[i]) * (A[i] - Bc[i]);
   }
   double kab = std::exp(-a * b / p * ab2) * scale;
-  auto ca = cart_list(la), cb = cart_list(lb);
+  const auto &ca = cart_list(la), &cb = cart_list(lb);
   int ncb = (int)cb.size();
   int lbe = (kind == 1) ? lb + 2 : lb;
   hermite_e(la, lbe, p, P[0] - A[0], P[0] - Bc[0], w.ex);
@@ -862,7 +1178,7 @@ int orc_grad1e(const orc_basis *b, const double *dmat, const double *wmat, doubl
       for (int bb = 0; bb < ns; ++bb) {
         const Shell &A = B.sh[a], &Bs = B.sh[bb];
         int na = ncart(A.l), nb = ncart(Bs.l);
-        auto La = cart_list(A.l);
+        const auto &La = cart_list(A.l);
         // derivative w.r.t. centre of A (the bra function); the ket-centre
         // derivative is covered by the (b,a) ordered pair of the full loop.
         // kinds: S (weight -W), T (weight D), V per nucleus (weight D).

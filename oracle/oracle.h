@@ -61,6 +61,24 @@ int orc_schwarz(const orc_basis *b, double *q /* nshell^2 */, int64_t *shell_l, 
 int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat,
              double *fmat, double hfxfac, double thrs);
 
+/* orc_fock with Dalton's direct-Fock density screening (IFTHRS < 16 turns it
+ * on): the SYMLOP quartet skip on Dalton's blocks (her2drv.F:2663-2733), the
+ * FCKTOL integral drop and the per-density Coulomb/exchange skips selected by
+ * the bits of ICEDIF (her2fck.F:84-90, 221-222, 446-466).  counts (may be
+ * NULL) receives 5 values: quartets evaluated, skipped by the screen, skipped
+ * because their density bound is exactly zero, density Coulomb parts
+ * dropped, density exchange parts dropped. */
+int orc_fock_screened(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
+                      double hfxfac, double thrs, int64_t ifthrs, int64_t icedif, int64_t *counts);
+
+/* Class-stratified timing of a J+K build (IFCTYP 13, hfxfac 1) for the CPU
+ * baseline: per class (lA lB|lC lD) of significant segmented quartets, a
+ * count and a timed evenly spaced sample; *est_seconds is the extrapolated
+ * time of the whole build (see oracle.cpp). */
+int orc_fock_class_sample(const orc_basis *b, const double *dmat, double thrs, double target_seconds, int maxcls,
+                          int64_t *cls_l, int64_t *cls_count, int64_t *cls_sample, double *cls_seconds, int *ncls,
+                          double *est_seconds, int64_t *total);
+
 /* Sampled J+K build (IFCTYP 13, hfxfac 1) over the bra pairs ab with
  * ab % stride == offset, for CPU-baseline timing; *nquartet = quartets done. */
 int orc_fock_sampled(const orc_basis *b, const double *dmat, double *fmat, double thrs, int stride, int offset,

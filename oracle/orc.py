@@ -54,6 +54,11 @@ def lib():
         _lib.orc_fock_sampled.argtypes = [ctypes.POINTER(OrcBasis), _dp, _dp, ctypes.c_double, ctypes.c_int,
                                           ctypes.c_int, _i64p]
         _lib.orc_schwarz.argtypes = [ctypes.POINTER(OrcBasis), _dp, _i64p, _i64p, _i64p]
+        _lib.orc_fock_screened.argtypes = [ctypes.POINTER(OrcBasis), ctypes.c_int, _i64p, _dp, _dp,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _i64p]
+        _lib.orc_fock_class_sample.argtypes = [ctypes.POINTER(OrcBasis), _dp, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_int, _i64p, _i64p, _i64p, _dp,
+                                               ctypes.POINTER(ctypes.c_int), _dp, _i64p]
     return _lib
 
 
@@ -132,6 +137,49 @@ def eri_full(bs) -> np.ndarray:
     out = np.zeros(n ** 4)
     lib().orc_eri_full(ctypes.byref(h.s), _p(out, ctypes.c_double))
     return out.reshape(n, n, n, n)
+
+
+def fock_screened(bs, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, icedif=3):
+    """HERFCK-semantics Fock build with Dalton's density screening (IFTHRS,
+    ICEDIF; see oracle.h).  Returns (F, counts) with counts a dict of the
+    screening statistics."""
+    h = _Holder(bs)
+    d = np.ascontiguousarray(dmat, dtype=np.float64)
+    single = d.ndim == 2
+    if single:
+        d = d[None]
+    nd = d.shape[0]
+    ift = np.ascontiguousarray(np.broadcast_to(np.asarray(ifctyp, dtype=np.int64), (nd,)))
+    f = np.zeros_like(d)
+    c = np.zeros(5, dtype=np.int64)
+    lib().orc_fock_screened(ctypes.byref(h.s), nd, _p(ift, ctypes.c_int64), _p(d, ctypes.c_double),
+                            _p(f, ctypes.c_double), float(hfxfac), float(thrs), int(ifthrs), int(icedif),
+                            _p(c, ctypes.c_int64))
+    counts = dict(zip(("evaluated", "skipped_screen", "skipped_zero", "dropped_coulomb", "dropped_exchange"),
+                      (int(x) for x in c)))
+    return (f[0] if single else f), counts
+
+
+def fock_class_sample(bs, dmat, thrs=1e-12, target_seconds=10.0):
+    """Class-stratified timing of the J+K build (see oracle.h): returns a dict
+    with the extrapolated seconds of the whole build, the quartet count and a
+    per-class table."""
+    h = _Holder(bs)
+    d = np.ascontiguousarray(dmat, dtype=np.float64)
+    maxcls = 512
+    cl = np.zeros(4 * maxcls, dtype=np.int64)
+    cc, cs = np.zeros(maxcls, dtype=np.int64), np.zeros(maxcls, dtype=np.int64)
+    sec = np.zeros(maxcls)
+    n = ctypes.c_int()
+    est = ctypes.c_double()
+    tot = ctypes.c_int64()
+    lib().orc_fock_class_sample(ctypes.byref(h.s), _p(d, ctypes.c_double), float(thrs), float(target_seconds), maxcls,
+                                _p(cl, ctypes.c_int64), _p(cc, ctypes.c_int64), _p(cs, ctypes.c_int64),
+                                _p(sec, ctypes.c_double), ctypes.byref(n), ctypes.byref(est), ctypes.byref(tot))
+    k = min(n.value, maxcls)
+    classes = [{"class": [int(x) for x in cl[4 * i:4 * i + 4]], "count": int(cc[i]), "sample": int(cs[i]),
+                "sample_seconds": float(sec[i])} for i in range(k)]
+    return {"est_seconds": est.value, "quartets": int(tot.value), "classes": classes}
 
 
 def fock(bs, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12) -> np.ndarray:

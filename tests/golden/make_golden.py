@@ -1,15 +1,17 @@
 """Regenerate dalton_energies.json from Dalton's stored test outputs.
 
-Reads the golden numbers as text from a Dalton source tree (default
-/root/reference) and writes them, with their file:line provenance, into
+Reads the golden numbers as text from a Dalton source tree (its path is the
+one argument) and writes them, with their file:line provenance, into
 tests/golden/dalton_energies.json.  The tests read only the JSON.
+
+    python tests/golden/make_golden.py <path to a Dalton source tree>
 """
 import json
 import os
 import re
 import sys
 
-SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+SRC = sys.argv[1] if len(sys.argv) > 1 else None
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "dalton_energies.json")
 
 
@@ -51,4 +53,6 @@ def main():
 
 
 if __name__ == "__main__":
+    if SRC is None:
+        sys.exit("usage: make_golden.py <path to a Dalton source tree>")
     main()
