@@ -32,9 +32,8 @@ sys.path.insert(0, ROOT)
 METRIC = "J+K build ms & ERI quartets/s, mixed vs FP64 at <=1e-6 Eh; HF gradient ms"
 MIXED_CUTOFF = 1e-6
 THRS = 1e-12
-# dgf_class_time.kernel: thread-per-quartet, cooperative team, warp teams, thread-per-quartet with the density
-# tile, warp-per-quartet
-KERNEL_KIND = ("thread", "team", "team", "thread", "warp")
+# dgf_class_time.kernel: 0 thread-per-quartet, 1 cooperative team, 2 warp teams, 4 warp-per-quartet
+KERNEL_KIND = {0: "thread", 1: "team", 2: "team", 4: "warp"}
 
 
 def parse():
@@ -148,12 +147,12 @@ def dist_setup(args):
     return world, rank, local
 
 
-def cpu_baseline_sample(bs, dmat, target_s, threads=0):
-    """Oracle (CPU restatement of Dalton's HERMIT J+K) timed class by class:
-    every quartet class of the workload is counted, an evenly spaced sample
-    of each class is evaluated and digested on all host cores, and the whole
-    build's time is the sum of count x sampled seconds per quartet
-    (class-stratified, so the class mix is the workload's own)."""
+def cpu_baseline_sample(bs, dmat, target_s, threads=0, k=None):
+    """Oracle (CPU restatement of Dalton's HERMIT J+K) on a fixed
+    pseudo-random subset of the workload's significant quartets (hash-selected,
+    so the class mix is the workload's), all host cores; the sampling
+    fraction 2^-k is chosen from a short calibration run so that the sample
+    takes target_s to 2 target_s seconds, unless k is given."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import orc
 
@@ -161,19 +160,21 @@ def cpu_baseline_sample(bs, dmat, target_s, threads=0):
     if threads:
         orc.set_threads(threads)
     cores = orc.threads()
-    t0 = time.perf_counter()
-    r = orc.fock_class_sample(bs, dmat, THRS, target_s)
-    wall = time.perf_counter() - t0
-    rate = r["quartets"] / r["est_seconds"]
-    nsample = sum(c["sample"] for c in r["classes"])
+    if k is None:
+        k0 = 16
+        n, sec, tot = orc.fock_hash_sample(bs, dmat, k0, THRS)
+        est_full = tot * sec / max(n, 1)
+        k = max(0, min(30, int(np.floor(np.log2(max(est_full / max(target_s, 1e-3), 1.0))))))
+    n, sec, tot = orc.fock_hash_sample(bs, dmat, k, THRS)
+    rate = n / sec
     return {"value": rate, "unit": "quartets/s", "cores": cores, "kind": "port",
             "sample": f"oracle J+K (C++ restatement of Dalton's HERMIT McMurchie-Davidson build and FCKCON "
-                      f"digestion; Dalton itself needs gfortran, absent here) timed class by class: "
-                      f"{len(r['classes'])} quartet classes, {nsample} sampled quartets of {r['quartets']}, "
-                      f"extrapolated full build {r['est_seconds']:.1f} s on {cores} threads; unlike HERMIT it "
-                      f"evaluates general contractions (cc-pVDZ O 1s/2s, H 1s) as separate segmented shells, "
-                      f"so it repeats their primitive integrals",
-            "est_full_build_s": r["est_seconds"], "quartets": r["quartets"], "wall_s": wall}
+                      f"digestion; Dalton itself needs gfortran, absent here) on a fixed hash-selected 2^-{k} "
+                      f"subset of the workload's {tot} significant quartets ({n} quartets, all classes in the "
+                      f"workload's proportions) in {sec:.2f} s on {cores} threads, i.e. a full build of "
+                      f"{tot / rate:.0f} s; unlike HERMIT it evaluates general contractions (cc-pVDZ O 1s/2s, "
+                      f"H 1s) as separate segmented shells, so it repeats their primitive integrals",
+            "k": k, "est_full_build_s": tot / rate, "quartets": tot, "seconds": sec}
 
 
 def workload_config(name, bs, mol, basis):
@@ -208,9 +209,11 @@ def run_reference(args):
     per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
     vals = []
     info = None
-    for k in range(args.warmup + args.steps):
-        info = cpu_baseline_sample(bs, d, per_step)
-        if k >= args.warmup:
+    k = None  # sampling fraction fixed by the first step's calibration
+    for step in range(args.warmup + args.steps):
+        info = cpu_baseline_sample(bs, d, per_step, k=k)
+        k = info["k"]
+        if step >= args.warmup:
             vals.append(info["value"])
     v = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "quartets/s", "n_gpus": args.gpus,
@@ -684,9 +687,29 @@ def main():
         gfull = rhf_gradient(gfb, Dg, gscf["wmat"], thrs=THRS)
         torch.cuda.synchronize(dev)
         full_ms = (time.perf_counter() - t0) * 1e3
+        # roofline of the backward kernels: one profiled call, per-class device times
+        from dalton_b200.perfmodel import grad_class_flops
+
+        gfb.set_profiling(True)
+        grad2e_bilinear(gfb, Dg, Dg, 1.0, THRS)
+        gprof = gfb.profile()
+        gfb.set_profiling(False)
+        gtop = max(gprof, key=lambda r: r["ms"])
+        gflops = grad_class_flops(gtop["la"], gtop["lb"], gtop["lc"], gtop["ld"], gtop["prim_quartets"],
+                                  gtop["evaluated"])
+        gall = sum(grad_class_flops(r["la"], r["lb"], r["lc"], r["ld"], r["prim_quartets"], r["evaluated"])
+                   for r in gprof)
+        gms = sum(r["ms"] for r in gprof)
+        g_roof = {"kernel": f"grad_thread_kernel<{gtop['la']},{gtop['lb']},{gtop['lc']},{gtop['ld']}>",
+                  "ms": gtop["ms"], "share": gtop["ms"] / gms if gms else None,
+                  "achieved_tflops": gflops / (gtop["ms"] * 1e-3) / 1e12,
+                  "frac": gflops / (gtop["ms"] * 1e-3) / 1e12 / fp64_peak,
+                  "all_kernels_tflops": gall / (gms * 1e-3) / 1e12 if gms else None,
+                  "flops_model": "dalton_b200/perfmodel.py grad_class_flops"}
         grad_info = {"workload": f"h2o16_ccpvdz: (H2O)16 cluster, {gbas}, {gbs.nbf} basis functions, RHF "
                                  f"converged to 1e-8 ({gscf['niter']} iterations)",
                      "grad2e_ms": g2_ms, "full_gradient_ms": full_ms, "energy": gscf["energy"],
+                     "roofline": g_roof,
                      "max_abs_gradient": float(np.abs(gfull).max()),
                      "translational_sum": float(np.abs(gfull.sum(0)).max())}
         gfb.close()
@@ -700,8 +723,8 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(bs, D.cpu().numpy(), args.cpu_seconds)
-        cpu.pop("seconds", None)
-        cpu.pop("quartets", None)
+        for key in ("seconds", "quartets", "k"):
+            cpu.pop(key, None)
 
     if rank == 0:
         line = {

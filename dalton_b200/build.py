@@ -78,7 +78,7 @@ def _generated_units():
     gen = os.path.join(BUILD, "gen")
     os.makedirs(gen, exist_ok=True)
     units = []
-    for kind, header, macro, n, parts in (("jk", "dgf_jk_inst.cuh", "DGF_JK_CLASS", NUM_PAIR_CLASS, 3),
+    for kind, header, macro, n, parts in (("jk", None, None, NUM_PAIR_CLASS, 3),
                                           ("grad", "dgf_grad_kernel.cuh", "DGF_GRAD_CLASS", NUM_GRAD_CLASS, 0)):
         for x in range(n):
             for y in range(x + 1):
@@ -86,9 +86,12 @@ def _generated_units():
                     if part is None:
                         path = os.path.join(gen, f"dgf_{kind}_{x}_{y}.cu")
                         text = f'#include "{header}"\n\n{macro}({x}, {y})\n'
-                    else:
+                    elif part == 0:  # cooperative, warp-team and warp-per-quartet kernels
+                        path = os.path.join(gen, f"dgf_{kind}_{x}_{y}_0.cu")
+                        text = f'#include "dgf_jk_inst_team.cuh"\n\nDGF_JK_TEAM_CLASS({x}, {y})\n'
+                    else:  # thread kernels, FP64 (1) or FP32 (2)
                         path = os.path.join(gen, f"dgf_{kind}_{x}_{y}_{part}.cu")
-                        text = f'#include "{header}"\n\n{macro}({x}, {y}, {part})\n'
+                        text = f'#include "dgf_jk_inst_thread.cuh"\n\nDGF_JK_THREAD_CLASS({x}, {y}, {part})\n'
                     if not os.path.exists(path) or open(path).read() != text:
                         with open(path, "w") as f:
                             f.write(text)

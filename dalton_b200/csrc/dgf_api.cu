@@ -182,7 +182,7 @@ static void free_ctx(dgf_ctx *c) {
   cudaSetDevice(c->device);
   void *ptrs[] = {c->d_pairs, c->d_pp,     c->d_boys,   c->d_sph,   c->d_D,     c->d_Ds,    c->d_Fh, c->d_io,
                   c->d_dmax,  c->d_cnt,    c->d_qoff,   c->d_wmap_i, c->d_wmap_c, c->d_wmeta, c->d_wdims, c->d_gw,
-                  c->d_shinfo, c->d_blk_gab, c->d_blk_info, c->d_blk_dmax};
+                  c->d_shinfo, c->d_blk_gab, c->d_blk_info, c->d_blk_dmax, c->d_ks_i, c->d_ks_q, c->d_ks_pp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -225,25 +225,6 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
   if (nq <= 0 && !args.diag_out) return DGF_OK;
   int64_t grid64 = std::min<int64_t>((nq + per_block - 1) / per_block, (int64_t)c->nsm * (thread_kernel ? 8 : 16));
   int grid = (int)std::max<int64_t>(grid64, 1);
-  // Tiled digestion: one density slot, bra rows that fit in shared memory,
-  // and long enough runs of kets per bra for the tile flushes to pay.
-  size_t smem = k.smem;
-  args.tile_rows = args.tile_fa = args.tile_n = 0;
-  if (thread_kernel && c->tile_enabled && args.nslot == 1 && !args.kbase && !args.diag_out && k.occ) {
-    const int la = cls_l1(X), lb = X - la * (la + 1) / 2;
-    const int fa = nfun(la, c->spherical), fb = nfun(lb, c->spherical);
-    const size_t bytes = (size_t)(fa + fb) * c->nwf * sizeof(double);
-    if (bytes <= kTileMaxBytes && nq >= kTileMinQuartetsPerBra * (int64_t)args.nbra) {
-      const int occ = k.occ(bytes);
-      if (occ > 0) {
-        args.tile_rows = fa + fb;
-        args.tile_fa = fa;
-        args.tile_n = c->nwf;
-        smem = bytes;
-        grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->nsm * occ, (nq + 255) / 256));
-      }
-    }
-  }
   const bool prof = c->profiling && !args.diag_out;
   if (prof) {
     cudaEvent_t e0, e1;
@@ -253,7 +234,7 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
     c->prof_ev.push_back(e1);
     DGF_CUDA_CHECK(cudaEventRecord(e0, st));
   }
-  k.launch(args, grid, k.block, smem, st);
+  k.launch(args, grid, k.block, k.smem, st);
   DGF_CUDA_CHECK(cudaGetLastError());
   if (prof) {
     DGF_CUDA_CHECK(cudaEventRecord(c->prof_ev.back(), st));
@@ -263,7 +244,7 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
     r.lc = cls_l1(Y);
     r.ld = Y - r.lc * (r.lc + 1) / 2;
     r.precision = (precision == 1) ? 32 : 64;
-    r.kernel = thread_kernel ? (args.tile_rows ? 3 : 0) : k.kind == kKindWarpTeam ? 2 : k.kind == kKindWarp ? 4 : 1;
+    r.kernel = thread_kernel ? 0 : k.kind == kKindWarpTeam ? 2 : k.kind == kKindWarp ? 4 : 1;
     (void)k;
     r.quartets = args.nquartet - args.q_begin;
     r.evaluated = 0;
@@ -274,7 +255,11 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
   return DGF_OK;
 }
 
-static int finish_profile(dgf_ctx *c, cudaStream_t st) {
+int dgf_finish_profile(dgf_ctx *c, cudaStream_t st);
+static int finish_profile(dgf_ctx *c, cudaStream_t st) { return dgf_finish_profile(c, st); }
+
+// Waits for the profiled launches of the last call and stores their device times.
+int dgf_finish_profile(dgf_ctx *c, cudaStream_t st) {
   if (!c->profiling) return DGF_OK;
   DGF_CUDA_CHECK(cudaStreamSynchronize(st));
   for (size_t i = 0; i < c->prof.size(); ++i) {
@@ -644,10 +629,6 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
   if (device < 0 || device >= ndev) DGF_FAIL(DGF_ERR_ARG, "device index out of range");
   std::unique_ptr<dgf_ctx, void (*)(dgf_ctx *)> c(new dgf_ctx, free_ctx);
   c->device = device;
-  {
-    const char *nt = getenv("DGF_NO_TILE");
-    c->tile_enabled = !(nt && nt[0] == '1');
-  }
   DeviceGuard g(device);
   cudaDeviceProp prop;
   DGF_CUDA_CHECK(cudaGetDeviceProperties(&prop, device));
@@ -777,6 +758,28 @@ extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
   DGF_CUDA_CHECK(cudaMemcpy(c->d_pp, c->pp.data(), c->pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice));
   DGF_CUDA_CHECK(
       cudaMemcpy(c->d_pairs, c->pairs.data(), c->pairs.size() * sizeof(PairRec), cudaMemcpyHostToDevice));
+  // Ket table of single-primitive kets (first primitive pair of every pair).
+  if (c->nwshell < 65536 && !c->pairs.empty()) {
+    const size_t np = c->pairs.size();
+    std::vector<int4> ki(np);
+    std::vector<double> kq(np), kp(11 * np);
+    for (size_t g = 0; g < np; ++g) {
+      const PairRec &r = c->pairs[g];
+      ki[g] = make_int4(r.aoA, r.aoB, r.same, (r.shA << 16) | r.shB);
+      kq[g] = r.Q;
+      const PrimPair &q = c->pp[r.pp0];
+      const double v[11] = {q.p, q.Px, q.Py, q.Pz, q.K, q.PAx, q.PAy, q.PAz, q.PBx, q.PBy, q.PBz};
+      for (int k = 0; k < 11; ++k) kp[k * np + g] = v[k];
+    }
+    if (dev_alloc(&c->d_ks_i, np) != cudaSuccess || dev_alloc(&c->d_ks_q, np) != cudaSuccess ||
+        dev_alloc(&c->d_ks_pp, 11 * np) != cudaSuccess) {
+      cudaGetLastError();
+      DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the ket table failed");
+    }
+    DGF_CUDA_CHECK(cudaMemcpy(c->d_ks_i, ki.data(), np * sizeof(int4), cudaMemcpyHostToDevice));
+    DGF_CUDA_CHECK(cudaMemcpy(c->d_ks_q, kq.data(), np * 8, cudaMemcpyHostToDevice));
+    DGF_CUDA_CHECK(cudaMemcpy(c->d_ks_pp, kp.data(), 11 * np * 8, cudaMemcpyHostToDevice));
+  }
   *out = c.release();
   return DGF_OK;
 }
@@ -855,6 +858,17 @@ extern "C" int dgf_count_ao_quartets(dgf_ctx *c, double thrs, dgf_int *count) {
 static int ket_pp0_of(const dgf_ctx *c, const ClassPlan &cp) {
   if (cp.bucket != 0 || cp.kb1 <= cp.kb0) return -1;
   return c->pairs[c->cls_off[cp.Y] + cp.kb0].pp0;
+}
+
+// Ket-table arguments of a plan entry: set for entries whose kets have one
+// primitive pair each (bucket 0), cleared otherwise.
+static void set_ket_table(const dgf_ctx *c, const ClassPlan &cp, JKArgs &a) {
+  const bool on = c->d_ks_i && cp.bucket == 0 && cp.kb1 > cp.kb0;
+  a.ks_i = on ? c->d_ks_i : nullptr;
+  a.ks_q = on ? c->d_ks_q : nullptr;
+  a.ks_pp = on ? c->d_ks_pp : nullptr;
+  a.ks_stride = (int64_t)c->pairs.size();
+  a.ks_base = c->cls_off[cp.Y] + cp.kb0;
 }
 
 static int build_plan(dgf_ctx *c, double thrs) {
@@ -1239,6 +1253,7 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
       a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
       a.ket_off = cp.kb0;
       a.ket_pp0 = ket_pp0_of(c, cp);
+      set_ket_table(c, cp, a);
       a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
       a.same_class = (cp.X == cp.Y);
       a.qoff = c->d_qoff + cp.off;
@@ -1414,24 +1429,32 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
     a.q_begin = 0;
     const int la = cls_l1(cp.X), lb = cp.X - la * (la + 1) / 2, lc = cls_l1(cp.Y), ld = cp.Y - lc * (lc + 1) / 2;
     a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
+    float best_prec[2] = {1e30f, 1e30f};
     for (int p = 0; p < 2; ++p) {
       float best = 1e30f;
       int bestv = c->choice[cp.X][cp.Y][p];
       a.boys = c->d_boys + (p ? boys_low_offset(la + lb + lc + ld) : (size_t)(la + lb + lc + ld) * kBoysTableDoubles);
       const bool bra1 = c->cls_max_npp[cp.X] == 1;
+      // With the warp-per-quartet kernel available for the class's
+      // single-primitive launches, the cooperative kernels are not timed
+      // (they are several times slower wherever both exist).
+      const bool has_warp = bra1 && jk_kernel_variant(cp.X, cp.Y, p, -3, true, bra1).launch != nullptr;
       for (int v = -3; v < kThreadVariants; ++v) {
         if (!jk_kernel_variant(cp.X, cp.Y, p, v, false, bra1).launch &&
             !jk_kernel_variant(cp.X, cp.Y, p, v, true, bra1).launch)
           continue;
+        if (has_warp && (v == -1 || v == -2)) continue;
         int chunks = 1;
         float ms = 0.f;
-        for (int rep2 = 0; rep2 < 2; ++rep2) {  // first pass warms caches
+        for (int rep2 = 0; rep2 < 2; ++rep2) {  // a first pass warms caches unless it is long
+          if (rep2 == 1 && ms > 20.f) break;
           DGF_CUDA_CHECK(cudaEventRecord(e0, st));
           for (size_t q = ip; q < jp; ++q) {
             const ClassPlan &cq = c->plan[q];
             a.ket = c->d_pairs + c->cls_off[cq.Y] + cq.kb0;
             a.ket_off = cq.kb0;
             a.ket_pp0 = ket_pp0_of(c, cq);
+            set_ket_table(c, cq, a);
             a.qoff = c->d_qoff + cq.off;
             a.nquartet = cq.nquartet;
             // entries this candidate has no kernel for run the FP64 default (same for every candidate)
@@ -1455,21 +1478,27 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
         }
       }
       c->choice[cp.X][cp.Y][p] = bestv;
+      best_prec[p] = best;
     }
     // Mixed form: split the class into FP64 and FP32 launches only where
     // that beats one FP64 pass (both walk all of the class's quartets).
-    if (o.mixed_cutoff > 0.0 &&
+    // The split runs an FP64 and an FP32 launch over the whole queue; it can
+    // only win when the FP32 kernel is faster than the FP64 one.
+    if (o.mixed_cutoff > 0.0) c->split_ok[cp.X][cp.Y] = 0;
+    if (o.mixed_cutoff > 0.0 && best_prec[1] < best_prec[0] &&
         (select_kernel(c, cp.X, cp.Y, 1, false).launch || select_kernel(c, cp.X, cp.Y, 1, true).launch)) {
       const int Lq = la + lb + lc + ld;
       float t[2] = {0.f, 0.f};
       for (int cfg = 0; cfg < 2; ++cfg) {  // 0: FP64 only, 1: FP64 + FP32 halves
         for (int rep2 = 0; rep2 < 2; ++rep2) {
+          if (rep2 == 1 && t[cfg] > 20.f) break;
           DGF_CUDA_CHECK(cudaEventRecord(e0, st));
           for (size_t q = ip; q < jp; ++q) {
             const ClassPlan &cq = c->plan[q];
             a.ket = c->d_pairs + c->cls_off[cq.Y] + cq.kb0;
             a.ket_off = cq.kb0;
             a.ket_pp0 = ket_pp0_of(c, cq);
+            set_ket_table(c, cq, a);
             a.qoff = c->d_qoff + cq.off;
             a.nquartet = cq.nquartet;
             a.dmax = c->d_dmax;

@@ -66,6 +66,10 @@ struct dgf_ctx {
   int cls_max_npp[dgf::kNumPairClass] = {};     // most primitive pairs of a class's pairs
   std::vector<dgf::PrimPair> pp;
   dgf::PairRec *d_pairs = nullptr;
+  // ket table of single-primitive kets (JKArgs::ks_*), one entry per pair of
+  // d_pairs; null when a shell index does not fit 16 bits
+  int4 *d_ks_i = nullptr;
+  double *d_ks_q = nullptr, *d_ks_pp = nullptr;
   dgf::PrimPair *d_pp = nullptr;
   double *d_boys = nullptr, *d_sph = nullptr;
   // per-call buffers
@@ -83,7 +87,6 @@ struct dgf_ctx {
   int *d_blk_info = nullptr;
   float *d_blk_dmax = nullptr;
   int cap_blk_slots = 0;
-  int tile_enabled = 1;          // tiled digestion of the thread kernels (DGF_NO_TILE=1 turns it off)
   unsigned long long *d_cnt = nullptr;  // kCounterSlots x 4 per-launch counters
   // quartet plan, cached by Schwarz threshold
   double plan_thrs = -1.0;

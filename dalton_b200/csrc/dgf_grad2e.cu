@@ -37,7 +37,8 @@ GradLauncher g_grad_table[kGradClasses][kGradClasses];
 }  // namespace grad
 }  // namespace dgf
 
-int dgf_plan_for(dgf_ctx *c, double thrs);  // dgf_api.cu
+int dgf_plan_for(dgf_ctx *c, double thrs);         // dgf_api.cu
+int dgf_finish_profile(dgf_ctx *c, cudaStream_t st);  // dgf_api.cu
 
 static int grad_impl(dgf_ctx *c, const double *d1, const double *d2, double hfx, double thrs, double *grad,
                      cudaStream_t st) {
@@ -82,6 +83,15 @@ static int grad_impl(dgf_ctx *c, const double *d1, const double *d2, double hfx,
   a.natom = c->natom;
   a.schwarz_thr = thrs;
   a.ket_pp0 = -1;
+  // Per-launch profile (dgf_set_profiling): one record per class launch,
+  // kernel 5 = gradient; quartets are the plan's, primitive quartets from the
+  // classes' mean primitive-pair counts.
+  if (c->profiling) {
+    for (cudaEvent_t ev : c->prof_ev) cudaEventDestroy(ev);
+    c->prof_ev.clear();
+    c->prof.clear();
+  }
+  static const double kBucketPrims[kNumBuckets] = {1, 2, 4, 8, 16, 32, 64};
   for (const ClassPlan &cp : c->plan) {
     a.bra = c->d_pairs + c->cls_off[cp.X];
     a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
@@ -95,13 +105,37 @@ static int grad_impl(dgf_ctx *c, const double *d1, const double *d2, double hfx,
     a.boys = c->d_boys + (size_t)(L + 1) * kBoysTableDoubles;
     const int block = kGradBlock;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cp.nquartet + block - 1) / block, c->nsm * 8));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c->profiling) {
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      c->prof_ev.push_back(e0);
+      c->prof_ev.push_back(e1);
+      cudaEventRecord(e0, st);
+    }
     g_grad_table[cp.X][cp.Y](a, grid, block, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
       dgf::set_error(__FILE__, __LINE__, cudaGetErrorString(e));
       return DGF_ERR_CUDA;
     }
+    if (c->profiling) {
+      cudaEventRecord(e1, st);
+      dgf_class_time r;
+      r.la = cls_la(cp.X);
+      r.lb = cls_lb(cp.X);
+      r.lc = cls_la(cp.Y);
+      r.ld = cls_lb(cp.Y);
+      r.precision = 64;
+      r.kernel = 5;
+      r.quartets = r.evaluated = cp.nquartet;
+      const double bra = c->cls_avg_npp[cp.X] > 0 ? c->cls_avg_npp[cp.X] : 1.0;
+      r.prim_quartets = (int64_t)std::llround((double)cp.nquartet * bra * kBucketPrims[cp.bucket]);
+      r.ms = 0.0;
+      c->prof.push_back(r);
+    }
   }
+  if (c->profiling) return dgf_finish_profile(c, st);
   return DGF_OK;
 }
 

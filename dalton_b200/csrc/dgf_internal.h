@@ -134,10 +134,16 @@ struct JKArgs {
   int nblk;
   double ice_thr;
   int icedif;
-  // tiled digestion (thread kernels, one density slot, one molecule): the
-  // tile holds tile_fa rows of A and the rows of B of the block's bra pair,
-  // tile_n columns each, in dynamic shared memory; tile_rows = 0: no tile
-  int tile_rows, tile_fa, tile_n;
+  // ket table of single-primitive kets (kets of one primitive pair, one
+  // molecule): per pair index, {aoA, aoB, same, shA << 16 | shB}, the
+  // Schwarz factor, and the primitive pair's p, P, K, P-A, P-B as eleven
+  // planes of ks_stride doubles; ket ic of the launch is entry ks_base + ic.
+  // ks_i null: the kernels read the pair and primitive-pair records.
+  const int4 *ks_i;
+  const double *ks_q;
+  const double *ks_pp;
+  int64_t ks_stride;
+  int ks_base;
   // gradient mode (dgf_grad2e): densities D1, D2 (N*N) and grad (natom*3)
   const double *G1, *G2;
   double *grad;
@@ -155,26 +161,17 @@ __host__ __device__ inline int sph_offset(int l) {
 constexpr int kSphTableDoubles = 1 * 1 + 3 * 3 + 5 * 6 + 7 * 10 + 9 * 15;
 
 typedef void (*JKLauncher)(const JKArgs &, int grid, int block, size_t smem, cudaStream_t);
-// Resident blocks per SM of a kernel with `smem` bytes of dynamic shared memory.
-typedef int (*JKOccupancy)(size_t smem);
 
 enum { kKindThread = 0, kKindTeam = 1, kKindWarpTeam = 2, kKindWarp = 4 };
 
 struct ClassKernel {
   JKLauncher launch;
   int block;
-  size_t smem;   // dynamic shared memory (team kernels); 0 for thread kernels (plus the tile when tiled)
+  size_t smem;   // dynamic shared memory (team and warp kernels); 0 for thread kernels
   int chunks;    // thread kernels: A-component chunks (grid.y)
   int qpb;       // quartets a block works on at a time (grid sizing)
   int kind;      // kKindThread, kKindTeam, kKindWarpTeam or kKindWarp
-  JKOccupancy occ;  // thread kernels: occupancy query for tiled launches
 };
-
-// Tiled digestion of the thread kernels: largest tile (bytes of dynamic
-// shared memory), and the fewest quartets per bra pair for which a launch
-// uses it (the tile is flushed once per bra pair and block).
-constexpr size_t kTileMaxBytes = 96 * 1024;
-constexpr int64_t kTileMinQuartetsPerBra = 256;
 
 constexpr int kThreadVariants = 2;
 

@@ -1,8 +1,9 @@
 // Quartet-class kernel table of libdgfock: for every (bra class, ket class)
-// of angular momenta up to f, the cooperative team kernel and, for the
-// classes up to L = 5, register-resident thread kernels in FP64 and FP32,
-// each in two A-chunk variants (the per-class tuning space).  The entries
-// are filled by one generated translation unit per class pair (DGF_JK_CLASS).
+// of angular momenta up to f, the cooperative team kernel, the
+// warp-per-quartet kernel (L >= 4, FP64 and FP32) and, for the classes up to
+// L = 5, register-resident thread kernels in FP64 and FP32, each in two
+// A-chunk variants (the per-class tuning space).  The entries are filled by
+// generated translation units (dgf_jk_inst.cuh).
 #include "dgf_jk_inst.cuh"
 
 namespace dgf {
@@ -10,7 +11,7 @@ namespace dgf {
 JKEntry g_jk_table[kNumPairClass][kNumPairClass];
 
 namespace {
-const ClassKernel kNone{nullptr, 0, 0, 0, 0, 0, nullptr};
+const ClassKernel kNone{nullptr, 0, 0, 0, 0, 0};
 }
 
 // variant: -3 = warp-per-quartet kernel, -2 = warp-team kernel, -1 = team

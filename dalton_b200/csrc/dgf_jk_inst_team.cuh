@@ -1,0 +1,94 @@
+// Instantiation of part 0 of the quartet-class kernel table (see
+// dgf_jk_inst.cuh): the cooperative, warp-team and warp-per-quartet kernels.
+#pragma once
+
+#include "dgf_jk_inst.cuh"
+#include "dgf_jk_team.cuh"
+#include "dgf_jk_warp.cuh"
+
+namespace dgf {
+namespace jkinst {
+
+template <int LA, int LB, int LC, int LD, int WT>
+void launch_team(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
+  jk_team_kernel<LA, LB, LC, LD, WT><<<grid, block, smem, s>>>(a);
+}
+
+// Classes with the warp-per-quartet kernel: L >= 4 whose per-warp shared
+// memory fits one warp in 100 KB (every class up to (fd|fd), not (ff|..)
+// pairs with L >= 11).  Below L = 6 it is a candidate of the autotuner next
+// to the thread kernels.
+template <int LA, int LB, int LC, int LD>
+constexpr bool warp_eligible() {
+  if constexpr (LA + LB + LC + LD < 4) {
+    return false;
+  } else {
+    return wq::Shape<LA, LB, LC, LD, double>::smem(1) <= 100 * 1024;
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename T>
+void launch_warp(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
+  jk_warp_kernel<LA, LB, LC, LD, T><<<grid, block, smem, s>>>(a);
+}
+
+template <int LA, int LB, int LC, int LD, typename T>
+ClassKernel warp_entry() {
+  using W = wq::Shape<LA, LB, LC, LD, T>;
+  return ClassKernel{&launch_warp<LA, LB, LC, LD, T>, 32 * W::WPB, W::smem(W::WPB), 1, W::WPB, kKindWarp};
+}
+
+template <int LA, int LB, int LC, int LD, typename T>
+cudaError_t prepare_warp() {
+  using W = wq::Shape<LA, LB, LC, LD, T>;
+  return cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)W::smem(W::WPB));
+}
+
+template <int X, int Y>
+cudaError_t prepare_team() {
+  constexpr int LA = cls_la(X), LB = cls_lb(X), LC = cls_la(Y), LD = cls_lb(Y);
+  using TS = TeamShape<LA, LB, LC, LD>;
+  cudaError_t e = cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TS::smem());
+  if constexpr (TS::kWarpTeams > 0)
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(jk_team_kernel<LA, LB, LC, LD, TS::kWarpTeams>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::smem_w(TS::kWarpTeams));
+  if constexpr (warp_eligible<LA, LB, LC, LD>()) {
+    if (e == cudaSuccess) e = prepare_warp<LA, LB, LC, LD, double>();
+    if (e == cudaSuccess) e = prepare_warp<LA, LB, LC, LD, float>();
+  }
+  return e;
+}
+
+template <int X, int Y>
+void fill_team() {
+  constexpr int LA = cls_la(X), LB = cls_lb(X), LC = cls_la(Y), LD = cls_lb(Y);
+  using S = TeamShape<LA, LB, LC, LD>;
+  JKEntry &e = g_jk_table[X][Y];
+  e.prepare[0] = &prepare_team<X, Y>;
+  constexpr int work = S::NAB * S::NCD;
+  constexpr int block = work >= 512 ? 128 : work >= 64 ? 64 : 32;
+  e.team = ClassKernel{&launch_team<LA, LB, LC, LD, 0>, block, S::smem(), 1, 1, kKindTeam};
+  if constexpr (S::kWarpTeams > 0)
+    e.wteam = ClassKernel{&launch_team<LA, LB, LC, LD, S::kWarpTeams>, 32 * S::kWarpTeams,
+                          S::smem_w(S::kWarpTeams), 1, S::kWarpTeams, kKindWarpTeam};
+  if constexpr (warp_eligible<LA, LB, LC, LD>()) {
+    e.warp[0] = warp_entry<LA, LB, LC, LD, double>();
+    e.warp[1] = warp_entry<LA, LB, LC, LD, float>();
+  }
+}
+
+}  // namespace jkinst
+}  // namespace dgf
+
+// Static initialiser filling part 0 of entry (X, Y).
+#define DGF_JK_TEAM_CLASS(X, Y)                                                               \
+  namespace dgf {                                                                             \
+  namespace {                                                                                 \
+  struct TeamInit_##X##_##Y {                                                                 \
+    TeamInit_##X##_##Y() { jkinst::fill_team<X, Y>(); }                                       \
+  } g_team_init_##X##_##Y;                                                                    \
+  }                                                                                           \
+  }

@@ -18,7 +18,7 @@
 // Fock matrices) are FP64 in both.
 #pragma once
 
-#include "dgf_jk_team.cuh"
+#include "dgf_select.cuh"
 
 namespace dgf {
 
@@ -49,13 +49,11 @@ __device__ __forceinline__ void seg_end(int key, int lane, bool &head, int &end)
 // blocks of FCKCON (DALTON/abacus/herfckcon.F:66-80)
 //   J_ab += g Ds_cd,  J_cd += g Ds_ab,
 //   K_ac += g D_bd, K_ad += g D_bc, K_bc += g D_ad, K_bd += g D_ac.
-// The lanes whose bra pair is the group bra (the block's tile bra, or the
-// warp's first bra without a tile) sum J_ab with a warp reduction and K_ac,
+// The lanes whose bra pair is the group bra (the warp's first bra) sum J_ab
+// with a warp reduction and K_ac,
 // K_bc over runs of adjacent lanes with the same C shell (the kets of a
 // Schwarz bin are sorted by shell) with a segmented reduction, so that one
-// atomic serves the run.  The exchange blocks read the density rows of the
-// bra's functions; with a tile those rows come from shared memory (loaded
-// once per bra pair and block), else from global memory.  Density screening
+// atomic serves the run.  Density screening
 // per density (ICEDIF, DALTON/abacus/her2fck.F:221-222,446-466): with
 // ice_thr > 0, a lane whose quartet consists of whole Dalton blocks drops
 // its Coulomb part of density k when max(|D|_AB,|D|_CD) max|g| < ice_thr
@@ -63,8 +61,7 @@ __device__ __forceinline__ void seg_end(int key, int lane, bool &head, int &end)
 // does (bit 2), with the block maxima of the AO density.
 template <int FA, int FB, int FC, int FD>
 __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool work, int ib, int ic, int gib,
-                                          const PairRec &br, const PairRec &kt, int a_off, const double *dtile,
-                                          int tile_fa) {
+                                          const PairRec &br, const PairRec &kt, int a_off) {
   // Segmented reduction of K_ac and K_bc where it is cheap next to the atomics it saves.
   constexpr bool SEG = (FA + FB) * FC <= 18;
   const unsigned full = 0xffffffffu;
@@ -79,8 +76,6 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
   // Group: lanes on the group bra reduce their bra-row blocks together.
   const bool grp = work && ib == gib;
   const PairRec brg = load_pair_fock(a.bra + gib);
-  const double *dt = grp ? dtile : nullptr;  // the density tile serves group lanes only
-  const int tn = brg.nbfm;
   // Runs of group lanes with the same C shell (K_ac, K_bc); other lanes are runs of their own.
   bool head = true;
   int send = lane;
@@ -102,13 +97,9 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
     const double *Dsk = a.Ds + k * a.slot_stride + db;
     double *Fk = a.Fh + k * a.slot_stride + db;
     double *Fg = a.Fh + k * a.slot_stride + brg.dbase;
-    // Rows of the bra's functions in D: the tile (slot 0 only) or global memory.
-    auto dA = [&](int x, int col) -> double {
-      return dt ? dt[(size_t)(a_off + x) * tn + col] : Dk[(size_t)(br.aoA + a_off + x) * N + col];
-    };
-    auto dB = [&](int y, int col) -> double {
-      return dt ? dt[(size_t)(tile_fa + y) * tn + col] : Dk[(size_t)(br.aoB + y) * N + col];
-    };
+    // Rows of the bra's functions in D.
+    auto dA = [&](int x, int col) -> double { return Dk[(size_t)(br.aoA + a_off + x) * N + col]; };
+    auto dB = [&](int y, int col) -> double { return Dk[(size_t)(br.aoB + y) * N + col]; };
     double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
     if (ice) {
       const int4 bb = block_of_pair(a.bra + ib), kb = block_of_pair(a.ket + ic);
@@ -229,30 +220,13 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
   }
 }
 
-// Loads the density rows of bra `ib` (rows of A, then rows of B, tile_n
-// columns each, density slot 0) into the tile; every thread of the block
-// takes part, reading whole rows.
-__device__ __forceinline__ void tile_load(const JKArgs &a, double *tile, int rows, int fa, int ib) {
-  const PairRec br = load_pair_fock(a.bra + ib);
-  const int n = br.nbfm;
-  const double *D = a.D + br.dbase;
-  for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
-    const int r = e / n, col = e - r * n;
-    const int row = r < fa ? br.aoA + r : br.aoB + (r - fa);
-    tile[e] = __ldg(D + (size_t)row * n + col);
-  }
-}
-
 constexpr int kThreadBlock = 256;
 constexpr int kThreadWarps = kThreadBlock / 32;
-// 32-quartet chunks each warp processes between two block synchronisations
-// of the tiled form.
-constexpr int kChunksPerSync = 2;
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, const double *sph, Tc *ebra,
-                                               double *tile, int *s_tib, unsigned long long &cnt_q,
-                                               unsigned long long &cnt_p, unsigned long long &cnt_s) {
+                                               unsigned long long &cnt_q, unsigned long long &cnt_p,
+                                               unsigned long long &cnt_s) {
   constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr int A0 = CH * NA / CA, A1 = (CH + 1) * NA / CA, NAc = A1 - A0;  // this chunk's A components
@@ -266,50 +240,16 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
   constexpr int NOUT = cmax(NACC, cmax(FAc, NAc) * cmax(NB, FBc) * cmax(NC, FCc) * cmax(ND, FDc));
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
-  // Each block takes one contiguous range of the queue; its warps work on
-  // consecutive 32-quartet chunks of it, kChunksPerSync chunks per warp per
-  // block iteration, so that the block stays on one bra pair for long runs
-  // (the tile of its bra rows).  A warp's chunks only move forward, so its
-  // bra index is found once by binary search and then by a short walk along
-  // qoff.
+  // Each block takes one contiguous range of the queue and its warps work
+  // on consecutive 32-quartet chunks of it, so that they usually share the
+  // bra pair; a warp's chunks only move forward, so its bra index is found
+  // once by binary search and then by a short walk along qoff.
   const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5;
-  const int64_t iter = (int64_t)32 * nw * kChunksPerSync;
   const int64_t nq = a.nquartet - a.q_begin;
   const int64_t bspan = ((nq + gridDim.x - 1) / gridDim.x + 31) & ~(int64_t)31;
   const int64_t bbegin = a.q_begin + (int64_t)blockIdx.x * bspan, bend = min(bbegin + bspan, a.nquartet);
-  const bool use_tile = tile != nullptr;
-  int ibw = -1;              // the warp's running bra
-  int tile_ib = -1, tib = -1;  // the block's tile bra; thread 0's running search for it
-  int parity = 0;
-  for (int64_t ibase = bbegin; ibase < bend; ibase += iter) {
-    if (use_tile) {
-      // Tile bra of this iteration: the bra of its last quartet (runs usually continue into the next one).
-      if (threadIdx.x == 0) {
-        const int64_t ql = min(ibase + iter, bend) - 1;
-        if (tib < 0) {
-          tib = find_bra(a.qoff, a.nbra, ql);
-        } else {
-          int steps = 0;
-          while (ql >= a.qoff[tib + 1] && steps < 32) {
-            ++tib;
-            ++steps;
-          }
-          if (ql >= a.qoff[tib + 1]) tib = find_bra(a.qoff, a.nbra, ql);
-        }
-        s_tib[parity] = tib;
-      }
-      __syncthreads();
-      const int nib = s_tib[parity];
-      parity ^= 1;
-      if (nib != tile_ib) {  // every warp has finished reading the previous tile (barrier above)
-        tile_load(a, tile, a.tile_rows, a.tile_fa, nib);
-        __syncthreads();
-        tile_ib = nib;
-      }
-    }
-    for (int jc = 0; jc < kChunksPerSync; ++jc) {
-    const int64_t base = ibase + ((int64_t)jc * nw + warp) * 32;
-    if (base >= bend) break;
+  int ibw = -1;  // the warp's running bra
+  for (int64_t base = bbegin + (int64_t)warp * 32; base < bend; base += (int64_t)nw * 32) {
     const int64_t q = base + lane;
     const bool active = q < bend;
     int ib0 = ibw;
@@ -339,9 +279,43 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
       if (q >= a.qoff[ib + 1]) ib = find_bra(a.qoff, a.nbra, q);
       ic = (int)(q - a.qoff[ib]) + (a.kbase ? a.kbase[ib] : 0);
       br = load_pair_fock(a.bra + ib);
-      kt = load_pair_fock(a.ket + ic);
-      // K1 with a known layout: the ket's primitive pair is fetched alongside its record
-      if (K1 && a.ket_pp0 >= 0) P2one = load_prim<(LC + LD > 0)>(a.pp + a.ket_pp0 + ic);
+      if (K1 && a.ks_i) {
+        // single-primitive kets from the ket table: whole coalesced fields
+        const int g = a.ks_base + ic;
+        const int4 ki = __ldg(a.ks_i + g);
+        kt.aoA = ki.x;
+        kt.aoB = ki.y;
+        kt.same = ki.z;
+        kt.shA = ki.w >> 16;
+        kt.shB = ki.w & 0xffff;
+        kt.pp0 = 0;
+        kt.npp = 1;
+        kt.nbfm = a.nbf;
+        kt.dbase = 0;
+        kt.Q = __ldg(a.ks_q + g);
+        const double *pl = a.ks_pp + g;
+        const int64_t S = a.ks_stride;
+        P2one.p = __ldg(pl);
+        P2one.Px = __ldg(pl + S);
+        P2one.Py = __ldg(pl + 2 * S);
+        P2one.Pz = __ldg(pl + 3 * S);
+        P2one.K = __ldg(pl + 4 * S);
+        P2one.ea = 0.0;
+        if (LC + LD > 0) {
+          P2one.PAx = __ldg(pl + 5 * S);
+          P2one.PAy = __ldg(pl + 6 * S);
+          P2one.PAz = __ldg(pl + 7 * S);
+          P2one.PBx = __ldg(pl + 8 * S);
+          P2one.PBy = __ldg(pl + 9 * S);
+          P2one.PBz = __ldg(pl + 10 * S);
+        } else {
+          P2one.PAx = P2one.PAy = P2one.PAz = P2one.PBx = P2one.PBy = P2one.PBz = 0.0;
+        }
+      } else {
+        kt = load_pair_fock(a.ket + ic);
+        // K1 with a known layout: the ket's primitive pair is fetched alongside its record
+        if (K1 && a.ket_pp0 >= 0) P2one = load_prim<(LC + LD > 0)>(a.pp + a.ket_pp0 + ic);
+      }
       sel = quartet_select(a, br, kt, a.bra + ib, a.ket + ic);
       if (sel == 2 && CH == 0 && a.mode != 2) ++cnt_s;  // a split class counts its skips in the FP64 launch
     }
@@ -349,7 +323,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
     Tc acc[NACC];
 #pragma unroll
     for (int k = 0; k < NACC; ++k) acc[k] = Tc(0);
-    if (K1 && work && a.ket_pp0 < 0) P2one = load_prim<(LC + LD > 0)>(a.pp + kt.pp0);
+    if (K1 && work && !a.ks_i && a.ket_pp0 < 0) P2one = load_prim<(LC + LD > 0)>(a.pp + kt.pp0);
     // Bra groups: lanes sharing a bra pair run its primitive loop together.
     unsigned pending = __ballot_sync(full, work);
     while (pending) {
@@ -541,24 +515,22 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
     }
     // Digestion with compile-time function counts (spherical or Cartesian).
     if (!__any_sync(full, work)) continue;
-    const int gib = use_tile ? tile_ib : ib0;
     if (sphr)
-      jk_digest<FAc, FBc, FCc, FDc>(a, g, work, ib, ic, gib, br, kt, 0, tile, a.tile_fa);
+      jk_digest<FAc, FBc, FCc, FDc>(a, g, work, ib, ic, ib0, br, kt, 0);
     else
-      jk_digest<NAc, NB, NC, ND>(a, g, work, ib, ic, gib, br, kt, A0, tile, a.tile_fa);
-    }
+      jk_digest<NAc, NB, NC, ND>(a, g, work, ib, ic, ib0, br, kt, A0);
   }
 }
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, const double *tab, const double *sph,
-                                                   Tc *ebra, double *tile, int *s_tib, unsigned long long &q,
-                                                   unsigned long long &p, unsigned long long &s) {
+                                                   Tc *ebra, unsigned long long &q, unsigned long long &p,
+                                                   unsigned long long &s) {
   if constexpr (CH < CA) {
     if (chunk == CH)
-      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, sph, ebra, tile, s_tib, q, p, s);
+      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, sph, ebra, q, p, s);
     else
-      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, sph, ebra, tile, s_tib, q, p, s);
+      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, sph, ebra, q, p, s);
   }
 }
 
@@ -583,17 +555,12 @@ __global__ void __launch_bounds__(kThreadBlock, thread_min_blocks(LA + LB + LC +
   __shared__ double tab[kBoysTableDoubles];
   __shared__ double sph[kSphTableDoubles];
   __shared__ Tc ebra_all[kThreadWarps][3 * EA];
-  __shared__ int s_tib[2];
-  // Tile of the density rows of the block's bra pair (tiled launches):
-  // tile_rows x tile_n doubles of dynamic shared memory.
-  extern __shared__ double tile_dyn[];
-  double *tile = a.tile_rows > 0 ? tile_dyn : nullptr;
   for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
   for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
   __syncthreads();
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
-  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, sph, ebra_all[threadIdx.x >> 5], tile, s_tib,
-                                                cnt_q, cnt_p, cnt_s);
+  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, sph, ebra_all[threadIdx.x >> 5], cnt_q, cnt_p,
+                                                cnt_s);
   if (a.counters) {
     const int lane = threadIdx.x & 31;
 #pragma unroll

@@ -1,6 +1,7 @@
 // Warp-per-quartet McMurchie-Davidson J/K kernel for the high angular
-// momentum classes (L = la+lb+lc+ld >= 6, up to (ff|fd)), where one thread
-// cannot hold a quartet's intermediates in registers.
+// momentum classes (L = la+lb+lc+ld >= 6, up to (fd|fd); also a tuning
+// candidate from L = 4), where one thread cannot hold a quartet's
+// intermediates in registers.
 //
 // Each warp of a block works through its own contiguous range of the class
 // queue, one quartet at a time; every index pattern is known at compile
@@ -11,13 +12,15 @@
 //                    R value is read once and applied to every ket
 //                    component that uses it, with the ket's Hermite
 //                    coefficient products E^cd_{tau nu phi} from a table
-//                    built per ket primitive pair          (C2, her2el2.F)
+//                    built per ket primitive pair (one term per lane, from
+//                    per-block index tables); components in register chunks
+//                                                          (C2, her2el2.F)
 //   (ab|cd)          bra transform, one ket component cd per lane, each X
 //                    value read once and applied to every bra component,
 //                    with the bra's product table (kept while consecutive
 //                    quartets share the bra)               (C1, her2el1.F)
-//   spherical        bra side per lane (register block), ket side per lane
-//                    over rows                             (C1SPHR/C2SPHR)
+//   spherical        index by index in shared memory, one output element
+//                    per lane                              (C1SPHR/C2SPHR)
 //   digestion        the six J/K blocks (FCKCON, herfckcon.F:66-80), one
 //                    output element per lane, FP64 atomics
 // Tc is the arithmetic type of R, the transforms and the tables (double:
@@ -27,7 +30,7 @@
 
 #include <utility>
 
-#include "dgf_jk_team.cuh"
+#include "dgf_select.cuh"
 
 namespace dgf {
 namespace wq {
@@ -79,6 +82,15 @@ constexpr int term_at(int la, int lb, int ij, int t, int u, int v) {
 
 constexpr int odd(int n) { return n | 1; }
 
+// Components per register chunk of the transforms.
+constexpr int kChunk = 36;
+// Whether any component pair of [i0, i0+n) uses Hermite index (t,u,v).
+constexpr bool chunk_uses(int la, int lb, int i0, int n, int t, int u, int v) {
+  for (int ij = i0; ij < i0 + n; ++ij)
+    if (uses(la, lb, ij, t, u, v)) return true;
+  return false;
+}
+
 // Calls f(std::integral_constant<int, i>) for i = 0 .. N-1, so that the loop
 // index is a constant expression inside f (index arithmetic and term
 // selection at compile time).
@@ -113,37 +125,55 @@ struct Shape {
   // six density blocks (double)
   static constexpr int RD = FAm * FBm + FCm * FDm + FAm * FCm + FAm * FDm + FBm * FCm + FBm * FDm;
   static constexpr int PER_WARP = RA + RB + RT + RD + 8;
-  // block-wide: Boys and spherical tables, packed (t,u,v), offsets of the product tables
-  static constexpr int COMMON = kBoysTableDoubles + kSphTableDoubles + (N3L + 1) / 2;
+  // block-wide: Boys and spherical tables, packed (t,u,v) positions, and the
+  // index tables of the bra and ket product tables (ints)
+  static constexpr int COMMON = kBoysTableDoubles + kSphTableDoubles + (N3L + TAB + TCD + 1) / 2;
   static constexpr size_t smem(int warps) { return ((size_t)COMMON + (size_t)warps * PER_WARP) * 8; }
   // warps per block: four when they fit in 100 KB, else two, else one
   static constexpr int WPB = smem(4) <= 100 * 1024 ? 4 : smem(2) <= 100 * 1024 ? 2 : 1;
 };
 
-// Cartesian -> spherical transform of one index of a register block
-// g[PRE][N][POST] -> o[PRE][M][POST], rows m of T (M x N) at T.
-template <int PRE, int N, int M, int POST>
-__device__ __forceinline__ void sph_index(const double *g, double *o, const double *T) {
+// One index of the Cartesian -> spherical transform of a block in shared
+// memory (rows ab = a*NB+b, columns cd = c*ND+d, row stride PG), lane-
+// parallel over the output elements; T is the M x N table of the index.
+// IDX 0: a (rows), 1: b (rows), 2: c (columns), 3: d (columns); NB1/ND1 are
+// the current sizes of the b and d indices, NA1/NC1 of a and c.
+template <int IDX, int N, int M, int NA1, int NB1, int NC1, int ND1, int PG>
+__device__ __forceinline__ void sph_pass(const double *in, double *out, const double *T, int lane) {
+  constexpr int NR = (IDX == 0 ? M : NA1) * (IDX == 1 ? M : NB1);  // output rows
+  constexpr int NCOL = (IDX == 2 ? M : NC1) * (IDX == 3 ? M : ND1);  // output columns
+  for (int e = lane; e < NR * NCOL; e += 32) {
+    const int r = e / NCOL, col = e - r * NCOL;
+    double s = 0.0;
+    if (IDX == 0) {
+      const int m = r / NB1, b = r - m * NB1;
 #pragma unroll
-  for (int i = 0; i < PRE; ++i)
+      for (int n = 0; n < N; ++n) s += T[m * N + n] * in[(n * NB1 + b) * PG + col];
+    } else if (IDX == 1) {
+      const int a = r / M, m = r - a * M;
 #pragma unroll
-    for (int m = 0; m < M; ++m)
+      for (int n = 0; n < N; ++n) s += T[m * N + n] * in[(a * NB1 + n) * PG + col];
+    } else if (IDX == 2) {
+      const int m = col / ND1, d = col - m * ND1;
 #pragma unroll
-      for (int j = 0; j < POST; ++j) {
-        double s = 0.0;
+      for (int n = 0; n < N; ++n) s += T[m * N + n] * in[r * PG + n * ND1 + d];
+    } else {
+      const int c = col / M, m = col - c * M;
 #pragma unroll
-        for (int n = 0; n < N; ++n) s += T[m * N + n] * g[(i * N + n) * POST + j];
-        o[(i * M + m) * POST + j] = s;
-      }
+      for (int n = 0; n < N; ++n) s += T[m * N + n] * in[r * PG + c * ND1 + n];
+    }
+    out[r * PG + col] = s;
+  }
 }
 
 }  // namespace wq
 
 // Post-processing and digestion of the Cartesian block Gc[ab][cd] (row
-// stride PG) of one quartet: spherical transform (SPH), then the six J/K
-// blocks.  Gs and Gf are scratch blocks of the warp; Db the density blocks.
+// stride PG) of one quartet: spherical transform (SPH, index by index
+// between Gc and the scratch block Gs), then the six J/K blocks; Db holds
+// the density blocks.
 template <int LA, int LB, int LC, int LD, typename Tc, bool SPH>
-__device__ __forceinline__ void wq_finish(const JKArgs &a, double *Gc, double *Gs, double *Gf, double *Db,
+__device__ __forceinline__ void wq_finish(const JKArgs &a, double *Gc, double *Gs, double *Db,
                                           const double *sph, const PairRec &br, const PairRec &kt, int ib, int ic,
                                           double w, int lane) {
   using S = wq::Shape<LA, LB, LC, LD, Tc>;
@@ -153,45 +183,31 @@ __device__ __forceinline__ void wq_finish(const JKArgs &a, double *Gc, double *G
   constexpr int FAB = FA * FB, FCD = FC * FD;
   const double *G = Gc;
   if (SPH) {
-    // bra side: one ket component cd per lane, Gc column -> Gs column
-    for (int cd = lane; cd < NCD; cd += 32) {
-      double g[NA * NB], t1[FA * NB], t2[FA * FB];
-#pragma unroll
-      for (int ab = 0; ab < NA * NB; ++ab) g[ab] = Gc[ab * PG + cd];
-      if (LA >= 2)
-        wq::sph_index<1, NA, FA, NB>(g, t1, sph + sph_offset(LA));
-      else
-#pragma unroll
-        for (int k = 0; k < NA * NB; ++k) t1[k] = g[k];
-      if (LB >= 2)
-        wq::sph_index<FA, NB, FB, 1>(t1, t2, sph + sph_offset(LB));
-      else
-#pragma unroll
-        for (int k = 0; k < FA * NB; ++k) t2[k] = t1[k];
-#pragma unroll
-      for (int ab = 0; ab < FAB; ++ab) Gs[ab * PG + cd] = t2[ab];
+    // index by index, ping-pong between Gc and Gs
+    constexpr int FA1 = LA >= 2 ? 2 * LA + 1 : NA, FB1 = LB >= 2 ? 2 * LB + 1 : NB;
+    constexpr int FC1 = LC >= 2 ? 2 * LC + 1 : NC;
+    double *src = Gc, *dst = Gs;
+    if constexpr (LA >= 2) {
+      wq::sph_pass<0, NA, FA1, NA, NB, NC, ND, PG>(src, dst, sph + sph_offset(LA), lane);
+      __syncwarp();
+      double *t = src; src = dst; dst = t;
     }
-    __syncwarp();
-    // ket side: one spherical bra row per lane, Gs row -> Gf row
-    for (int ab = lane; ab < FAB; ab += 32) {
-      double h[NC * ND], t1[FC * ND], t2[FC * FD];
-#pragma unroll
-      for (int cd = 0; cd < NCD; ++cd) h[cd] = Gs[ab * PG + cd];
-      if (LC >= 2)
-        wq::sph_index<1, NC, FC, ND>(h, t1, sph + sph_offset(LC));
-      else
-#pragma unroll
-        for (int k = 0; k < NC * ND; ++k) t1[k] = h[k];
-      if (LD >= 2)
-        wq::sph_index<FC, ND, FD, 1>(t1, t2, sph + sph_offset(LD));
-      else
-#pragma unroll
-        for (int k = 0; k < FC * ND; ++k) t2[k] = t1[k];
-#pragma unroll
-      for (int cd = 0; cd < FCD; ++cd) Gf[ab * PG + cd] = t2[cd];
+    if constexpr (LB >= 2) {
+      wq::sph_pass<1, NB, FB1, FA1, NB, NC, ND, PG>(src, dst, sph + sph_offset(LB), lane);
+      __syncwarp();
+      double *t = src; src = dst; dst = t;
     }
-    __syncwarp();
-    G = Gf;
+    if constexpr (LC >= 2) {
+      wq::sph_pass<2, NC, FC1, FA1, FB1, NC, ND, PG>(src, dst, sph + sph_offset(LC), lane);
+      __syncwarp();
+      double *t = src; src = dst; dst = t;
+    }
+    if constexpr (LD >= 2) {
+      wq::sph_pass<3, ND, 2 * LD + 1, FA1, FB1, FC1, ND, PG>(src, dst, sph + sph_offset(LD), lane);
+      __syncwarp();
+      double *t = src; src = dst; dst = t;
+    }
+    G = src;
   }
   // Largest integral for the per-density Coulomb/exchange screen (ICEDIF).
   bool ice = false;
@@ -290,43 +306,52 @@ __device__ __forceinline__ void wq_finish(const JKArgs &a, double *Gc, double *G
   }
 }
 
-// Compact table of Hermite coefficient products of a shell pair (la, lb):
-// for every Cartesian component pair ij and (t,u,v) it uses,
-// E_x[ix,jx,t] E_y[iy,jy,u] E_z[iz,jz,v] from the 1D tables E (3 x EN),
-// at wq::term_at; one component pair per lane.
-template <int LA, int LB, typename Tc>
-__device__ __forceinline__ void wq_product_table(const Tc *E, Tc *tab, int lane) {
+// Index table of the compact Hermite product table of a shell pair
+// (la, lb), built once per block: for term k (ordered by component pair ij,
+// then t, u, v as in wq::term_at), the positions of its three factors in the
+// 1D tables E (x: ix,jx,t; y; z), packed 10 bits each.
+template <int LA, int LB>
+__device__ __forceinline__ void wq_term_index(int *idx, int tid, int nt) {
   constexpr int NB = ncart(LB), NIJ = ncart(LA) * NB, LT = LA + LB + 1, EN = (LA + 1) * (LB + 1) * LT;
-  for (int ij = lane; ij < NIJ; ij += 32) {
-    int ix, iy, iz, jx, jy, jz;
+  for (int ij = tid; ij < NIJ; ij += nt) {
+    int ix, iy, iz, jx, jy, jz, off = 0;
     cart_decode(LA, ij / NB, ix, iy, iz);
     cart_decode(LB, ij % NB, jx, jy, jz);
-    int off = 0;
     for (int k = 0; k < ij; ++k) {
       int ax, ay, az, bx, by, bz;
       cart_decode(LA, k / NB, ax, ay, az);
       cart_decode(LB, k % NB, bx, by, bz);
       off += (ax + bx + 1) * (ay + by + 1) * (az + bz + 1);
     }
-    const Tc *ex = E + (ix * (LB + 1) + jx) * LT, *ey = E + EN + (iy * (LB + 1) + jy) * LT,
-             *ez = E + 2 * EN + (iz * (LB + 1) + jz) * LT;
+    const int bxp = (ix * (LB + 1) + jx) * LT, byp = EN + (iy * (LB + 1) + jy) * LT,
+              bzp = 2 * EN + (iz * (LB + 1) + jz) * LT;
     for (int t = 0; t <= ix + jx; ++t)
-      for (int u = 0; u <= iy + jy; ++u) {
-        const Tc exy = ex[t] * ey[u];
-        for (int v = 0; v <= iz + jz; ++v) tab[off++] = exy * ez[v];
-      }
+      for (int u = 0; u <= iy + jy; ++u)
+        for (int v = 0; v <= iz + jz; ++v) idx[off++] = (bxp + t) | ((byp + u) << 10) | ((bzp + v) << 20);
+  }
+}
+
+// Compact table of Hermite coefficient products of a shell pair:
+// tab[k] = E_x E_y E_z of term k, from the 1D tables E and the index table;
+// one term per lane and round.
+template <int NT, typename Tc>
+__device__ __forceinline__ void wq_product_table(const Tc *E, const int *idx, Tc *tab, int lane) {
+  for (int k = lane; k < NT; k += 32) {
+    const int p = idx[k];
+    tab[k] = E[p & 1023] * E[(p >> 10) & 1023] * E[p >> 20];
   }
 }
 
 template <int LA, int LB, int LC, int LD, typename Tc>
 __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
   using S = wq::Shape<LA, LB, LC, LD, Tc>;
-  constexpr int L = S::L, LAB = S::LAB, BOX = S::BOX, NAB = S::NAB, NCD = S::NCD, N3AB = S::N3AB,
+  constexpr int L = S::L, BOX = S::BOX, NAB = S::NAB, NCD = S::NCD, N3AB = S::N3AB,
                 N3CD = S::N3CD, N3L = S::N3L, EA = S::EA, EC = S::EC, PX = S::PX, PG = S::PG;
   extern __shared__ double sm[];
   double *tab = sm;
   double *sph = tab + kBoysTableDoubles;
   int *tuvt = (int *)(sph + kSphTableDoubles);
+  int *idx_ab = tuvt + N3L, *idx_cd = idx_ab + S::TAB;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   double *wbase = sm + S::COMMON + (size_t)warp * S::PER_WARP;
   double *regA = wbase, *regB = regA + S::RA;
@@ -334,7 +359,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
   double *Db = regB + S::RB + S::RT;
   Tc *R0 = (Tc *)regA, *R1 = R0 + BOX * BOX * BOX;
   Tc *X = (Tc *)regB;
-  double *Gc = regA, *Gs = regB, *Gf = regA;
+  double *Gc = regA, *Gs = regB;
 
   for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
   for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
@@ -343,6 +368,8 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
     tuv_decode(e, t, u, v);
     tuvt[e] = (t * BOX + u) * BOX + v;  // position of (t,u,v) in the R box
   }
+  wq_term_index<LA, LB>(idx_ab, threadIdx.x, blockDim.x);
+  wq_term_index<LC, LD>(idx_cd, threadIdx.x, blockDim.x);
   __syncthreads();
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
   // One contiguous range of the queue per warp.
@@ -389,7 +416,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
           herm_e<LA, LB, 1, Tc>(Tc(0.5 / P1.p), Tc(pa), Tc(pb), Eb + lane * EA);
         }
         __syncwarp();
-        wq_product_table<LA, LB, Tc>(Eb, Tb, lane);
+        wq_product_table<S::TAB, Tc>(Eb, idx_ab, Tb, lane);
         tb_bra = ib;
       }
       {
@@ -416,7 +443,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
           }
         }
         __syncwarp();
-        wq_product_table<LC, LD, Tc>(Ek, Tk, lane);
+        wq_product_table<S::TCD, Tc>(Ek, idx_cd, Tk, lane);
         // R_tuv, level n = L-1 .. 0 from level n+1, ping-pong between R0 and R1
         Tc *prev = R0, *cur = R1;
         if (lane == 0) prev[0] = Tc(Fs[L]);
@@ -449,42 +476,57 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
           cur = sw;
         }
         const Tc *R = prev;
-        // ket transform: lane = bra Hermite index, every ket component
+        // ket transform: lane = bra Hermite index, every ket component (in
+        // chunks of kChunk components, R re-read per chunk)
         for (int e = lane; e < N3AB; e += 32) {
           const int base = tuvt[e];
-          Tc xa[NCD];
+          wq::static_for<(NCD + wq::kChunk - 1) / wq::kChunk>([&](auto CH_) {
+            constexpr int c0 = decltype(CH_)::value * wq::kChunk;
+            constexpr int nc = NCD - c0 < wq::kChunk ? NCD - c0 : wq::kChunk;
+            Tc xa[nc];
 #pragma unroll
-          for (int cd = 0; cd < NCD; ++cd) xa[cd] = Tc(0);
-          wq::static_for<N3CD>([&](auto F_) {
-            constexpr int f = decltype(F_)::value;
-            constexpr int ft = wq::tuv_t(f), fu = wq::tuv_u(f), fv = wq::tuv_v(f);
-            const Tc r = R[base + (ft * BOX + fu) * BOX + fv];
-            wq::static_for<NCD>([&](auto CD_) {
-              constexpr int cd = decltype(CD_)::value;
-              if constexpr (wq::uses(LC, LD, cd, ft, fu, fv)) xa[cd] += Tk[wq::term_at(LC, LD, cd, ft, fu, fv)] * r;
+            for (int k = 0; k < nc; ++k) xa[k] = Tc(0);
+            wq::static_for<N3CD>([&](auto F_) {
+              constexpr int f = decltype(F_)::value;
+              constexpr int ft = wq::tuv_t(f), fu = wq::tuv_u(f), fv = wq::tuv_v(f);
+              if constexpr (wq::chunk_uses(LC, LD, c0, nc, ft, fu, fv)) {
+                const Tc r = R[base + (ft * BOX + fu) * BOX + fv];
+                wq::static_for<nc>([&](auto K_) {
+                  constexpr int cd = c0 + decltype(K_)::value;
+                  if constexpr (wq::uses(LC, LD, cd, ft, fu, fv))
+                    xa[cd - c0] += Tk[wq::term_at(LC, LD, cd, ft, fu, fv)] * r;
+                });
+              }
             });
-          });
 #pragma unroll
-          for (int cd = 0; cd < NCD; ++cd) X[cd * PX + e] = xa[cd];
+            for (int k = 0; k < nc; ++k) X[(c0 + k) * PX + e] = xa[k];
+          });
         }
         __syncwarp();
       }
-      // bra transform: lane = ket component, every bra component
+      // bra transform: lane = ket component, every bra component (in chunks)
       for (int cd = lane; cd < NCD; cd += 32) {
-        Tc acc[NAB];
+        wq::static_for<(NAB + wq::kChunk - 1) / wq::kChunk>([&](auto CH_) {
+          constexpr int a0 = decltype(CH_)::value * wq::kChunk;
+          constexpr int na = NAB - a0 < wq::kChunk ? NAB - a0 : wq::kChunk;
+          Tc acc[na];
 #pragma unroll
-        for (int ab = 0; ab < NAB; ++ab) acc[ab] = Tc(0);
-        wq::static_for<N3AB>([&](auto E_) {
-          constexpr int e = decltype(E_)::value;
-          constexpr int et = wq::tuv_t(e), eu = wq::tuv_u(e), ev = wq::tuv_v(e);
-          const Tc xv = X[cd * PX + e];
-          wq::static_for<NAB>([&](auto AB_) {
-            constexpr int ab = decltype(AB_)::value;
-            if constexpr (wq::uses(LA, LB, ab, et, eu, ev)) acc[ab] += Tb[wq::term_at(LA, LB, ab, et, eu, ev)] * xv;
+          for (int k = 0; k < na; ++k) acc[k] = Tc(0);
+          wq::static_for<N3AB>([&](auto E_) {
+            constexpr int e = decltype(E_)::value;
+            constexpr int et = wq::tuv_t(e), eu = wq::tuv_u(e), ev = wq::tuv_v(e);
+            if constexpr (wq::chunk_uses(LA, LB, a0, na, et, eu, ev)) {
+              const Tc xv = X[cd * PX + e];
+              wq::static_for<na>([&](auto K_) {
+                constexpr int ab = a0 + decltype(K_)::value;
+                if constexpr (wq::uses(LA, LB, ab, et, eu, ev))
+                  acc[ab - a0] += Tb[wq::term_at(LA, LB, ab, et, eu, ev)] * xv;
+              });
+            }
           });
-        });
 #pragma unroll
-        for (int ab = 0; ab < NAB; ++ab) Gc[ab * PG + cd] = (double)acc[ab];
+          for (int k = 0; k < na; ++k) Gc[(a0 + k) * PG + cd] = (double)acc[k];
+        });
       }
       __syncwarp();
     }
@@ -493,9 +535,9 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
       cnt_p += 1;
     }
     if (a.spherical)
-      wq_finish<LA, LB, LC, LD, Tc, true>(a, Gc, Gs, Gf, Db, sph, br, kt, ib, ic, w, lane);
+      wq_finish<LA, LB, LC, LD, Tc, true>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane);
     else
-      wq_finish<LA, LB, LC, LD, Tc, false>(a, Gc, Gs, Gf, Db, sph, br, kt, ib, ic, w, lane);
+      wq_finish<LA, LB, LC, LD, Tc, false>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane);
     __syncwarp();
   }
   if (lane == 0 && a.counters) {

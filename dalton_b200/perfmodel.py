@@ -57,3 +57,33 @@ def flops_per_contracted(la, lb, lc, ld, spherical=True) -> float:
 def class_flops(la, lb, lc, ld, prim_quartets, quartets, spherical=True) -> float:
     return prim_quartets * flops_per_primitive(la, lb, lc, ld) + quartets * flops_per_contracted(la, lb, lc, ld,
                                                                                                    spherical)
+
+
+# Two-electron gradient (backward kernel), one fixed count per class:
+# per primitive quartet the Boys function and R_tuv to L+1, and for each of
+# the three differentiated centres (A, B, C; D by translational invariance)
+# and each direction the ket and bra contractions with that centre's angular
+# momentum raised by one; per contracted quartet the density product (8 flops
+# per Cartesian integral) and its contraction with the nine derivative
+# blocks (2 flops each).
+def grad_flops_per_primitive(la, lb, lc, ld) -> float:
+    L = la + lb + lc + ld + 1
+    f = 40 + 3 * L + 3 * sum(n3(j) for j in range(1, L + 1))
+    for centre in range(3):
+        ls = [la, lb, lc, ld]
+        ls[centre] += 1
+        lab, lcd = ls[0] + ls[1], ls[2] + ls[3]
+        ket = 2 * n3(lab) * n3(lcd) * ncart(ls[2]) * ncart(ls[3])
+        bra = 2 * n3(lab) * ncart(ls[0]) * ncart(ls[1]) * ncart(ls[2]) * ncart(ls[3])
+        f += 3 * (ket + bra)
+    return float(f)
+
+
+def grad_flops_per_contracted(la, lb, lc, ld) -> float:
+    ncart4 = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
+    return float(8 * ncart4 + 2 * 9 * ncart4)
+
+
+def grad_class_flops(la, lb, lc, ld, prim_quartets, quartets) -> float:
+    return prim_quartets * grad_flops_per_primitive(la, lb, lc, ld) + quartets * grad_flops_per_contracted(la, lb, lc,
+                                                                                                            ld)

@@ -198,16 +198,19 @@ typedef struct {
   int32_t la, lb, lc, ld;   /* angular momenta of the class (ab|cd) */
   int32_t precision;        /* 64 = FP64, 32 = FP32 contraction */
   int32_t kernel;           /* 0 = thread-per-quartet, 1 = cooperative team, 2 = warp teams,
-                               3 = thread-per-quartet reading the bra's density rows from shared
-                               memory, 4 = warp-per-quartet (single primitive pairs, L >= 6) */
+                               4 = warp-per-quartet (single primitive pairs, L >= 4),
+                               5 = two-electron gradient (dgf_grad2e*: quartets are the plan's,
+                               primitive quartets estimated from the classes' mean primitive
+                               pairs) */
   int64_t quartets;         /* quartets of the class in the plan */
   int64_t evaluated;        /* quartets this launch evaluated */
   int64_t prim_quartets;    /* primitive quartets this launch evaluated */
   double ms;                /* device time of the launch */
 } dgf_class_time;
 
-/* Turn per-launch profiling of dgf_fock / dgf_fock_device on (1) or off (0).
- * While on, each call synchronises its stream at the end. */
+/* Turn per-launch profiling of dgf_fock / dgf_fock_device and of the
+ * two-electron gradient calls on (1) or off (0).  While on, each call
+ * synchronises its stream at the end. */
 int dgf_set_profiling(dgf_ctx *ctx, int on);
 
 /* Copy up to `max` records of the last profiled call; *count = records. */

@@ -773,18 +773,28 @@ static int fock_core(const orc_basis *b, int ndmat, const int64_t *ifctyp, const
   return 0;
 }
 
-// Class-stratified timing of the J+K build (IFCTYP 13, hfxfac 1, no density
-// screening) for the CPU baseline: the significant canonical quartets of the
-// segmented shells are counted per class (l_A l_B | l_C l_D); from each class
-// an evenly spaced sample is evaluated and digested (all threads), its
-// seconds per quartet are measured, and the full build's time is the sum
-// over classes of count x seconds per quartet.  Outputs per class (up to
-// maxcls): the four l values, the count, the sample size and the sample
-// seconds; *ncls = number of classes; *est_seconds = the extrapolated full
-// build, *total = all quartets.  target_seconds bounds the sampled work.
-int orc_fock_class_sample(const orc_basis *b, const double *dmat, double thrs, double target_seconds, int maxcls,
-                          int64_t *cls_l, int64_t *cls_count, int64_t *cls_sample, double *cls_seconds, int *ncls,
-                          double *est_seconds, int64_t *total) {
+// Timing sample of the J+K build (IFCTYP 13, hfxfac 1, no density
+// screening) for the CPU baseline: the significant canonical quartets
+// (ab|cd) of the segmented shells whose hash of (ab, cd) falls below
+// 2^(64 - k) -- a fixed pseudo-random subset of about 2^-k of the quartet
+// list, so its class mix is the workload's -- are evaluated and digested on
+// all threads.  *nsample receives the quartets evaluated, *seconds the wall
+// time of that evaluation (the selection scan, which a full build spends
+// about a nanosecond per quartet on, the Schwarz pre-pass and set-up
+// excluded), *total the number of significant quartets.  k = 0 evaluates
+// every quartet.
+static inline uint64_t quartet_hash(uint64_t ab, uint64_t cd) {
+  uint64_t x = ab * 0x9E3779B97F4A7C15ull ^ (cd + 0x632BE59BD9B4E019ull);
+  x ^= x >> 31;
+  x *= 0xD6E8FEB86659FD93ull;
+  x ^= x >> 32;
+  x *= 0xD6E8FEB86659FD93ull;
+  x ^= x >> 32;
+  return x;
+}
+
+int orc_fock_hash_sample(const orc_basis *b, const double *dmat, double thrs, int k, int64_t *nsample,
+                         double *seconds, int64_t *total) {
   set_threads();
   Basis B = make_basis(b);
   const int ns = (int)B.sh.size();
@@ -796,103 +806,49 @@ int orc_fock_class_sample(const orc_basis *b, const double *dmat, double thrs, d
   for (int a = 0; a < ns; ++a)
     for (int c = 0; c <= a; ++c) pairs.push_back({a, c});
   const int npair = (int)pairs.size();
-  const int L1 = B.maxl + 1;
-  auto key = [&](int a, int bq, int c, int d) {
-    return ((B.sh[a].l * L1 + B.sh[bq].l) * L1 + B.sh[c].l) * L1 + B.sh[d].l;
-  };
-  const int nkey = L1 * L1 * L1 * L1;
-  // counts per class
-  std::vector<int64_t> cnt(nkey, 0);
-#pragma omp parallel
+  const uint64_t cut = k <= 0 ? ~0ull : (k >= 64 ? 0ull : (~0ull >> k));
+  int64_t ntot = 0;
+  std::vector<std::pair<int, int>> smp;
+#pragma omp parallel reduction(+ : ntot)
   {
-    std::vector<int64_t> cl(nkey, 0);
+    std::vector<std::pair<int, int>> mine;
 #pragma omp for schedule(dynamic, 64)
-    for (int ab = 0; ab < npair; ++ab) {
-      const int sA = pairs[ab].first, sB = pairs[ab].second;
-      const double qab = Q[(size_t)sA * ns + sB];
-      for (int cd = 0; cd <= ab; ++cd) {
-        const int sC = pairs[cd].first, sD = pairs[cd].second;
-        if (qab * Q[(size_t)sC * ns + sD] >= thrs) ++cl[key(sA, sB, sC, sD)];
-      }
-    }
-#pragma omp critical
-    for (int k = 0; k < nkey; ++k) cnt[k] += cl[k];
-  }
-  // evenly spaced samples of at most smax quartets per class
-  auto collect = [&](const std::vector<int64_t> &want, std::vector<std::vector<std::pair<int, int>>> &out) {
-    out.assign(nkey, {});
-    std::vector<int64_t> stride(nkey, 1), seen(nkey, 0);
-    for (int k = 0; k < nkey; ++k) {
-      stride[k] = want[k] > 0 ? std::max<int64_t>(1, cnt[k] / want[k]) : 0;
-      if (want[k] > 0) out[k].reserve(want[k] + 1);
-    }
-    for (int ab = 0; ab < npair; ++ab) {
+    for (int ab = npair - 1; ab >= 0; --ab) {
       const int sA = pairs[ab].first, sB = pairs[ab].second;
       const double qab = Q[(size_t)sA * ns + sB];
       for (int cd = 0; cd <= ab; ++cd) {
         const int sC = pairs[cd].first, sD = pairs[cd].second;
         if (qab * Q[(size_t)sC * ns + sD] < thrs) continue;
-        const int k = key(sA, sB, sC, sD);
-        if (stride[k] && seen[k]++ % stride[k] == 0 && (int64_t)out[k].size() < want[k]) out[k].push_back({ab, cd});
+        ++ntot;
+        if (quartet_hash((uint64_t)ab, (uint64_t)cd) <= cut) mine.push_back({ab, cd});
       }
     }
-  };
-  auto run = [&](const std::vector<std::pair<int, int>> &smp) {
-    double t0 = omp_get_wtime();
-#pragma omp parallel
-    {
-      std::vector<double> Fl(N2, 0.0);
-      const double keep = 1.0;
-      EriWork w;
-      std::vector<double> g, cart, tmp;
-#pragma omp for schedule(dynamic, 4)
-      for (int64_t i = 0; i < (int64_t)smp.size(); ++i) {
-        const int ab = smp[i].first, cd = smp[i].second;
-        const int sA = pairs[ab].first, sB = pairs[ab].second, sC = pairs[cd].first, sD = pairs[cd].second;
-        shell_eri(B, sA, sB, sC, sD, g, w, cart, tmp);
-        digest_quartet(B, sA, sB, sC, sD, ab == cd, g, ds, 1, 0.5, &keep, &keep, -1.0, Fl.data());
-      }
-    }
-    return omp_get_wtime() - t0;
-  };
-  // calibration: a small sample per class gives seconds per quartet
-  int nclass = 0;
-  for (int k = 0; k < nkey; ++k) nclass += cnt[k] > 0;
-  std::vector<int64_t> want(nkey, 0);
-  for (int k = 0; k < nkey; ++k) want[k] = std::min<int64_t>(cnt[k], 256);
-  std::vector<std::vector<std::pair<int, int>>> smp;
-  collect(want, smp);
-  std::vector<double> spq(nkey, 0.0);
-  for (int k = 0; k < nkey; ++k)
-    if (!smp[k].empty()) spq[k] = run(smp[k]) / smp[k].size();
-  // main sample: each class gets an equal share of the time budget
-  const double share = target_seconds / std::max(nclass, 1);
-  for (int k = 0; k < nkey; ++k)
-    want[k] = cnt[k] ? std::min<int64_t>(cnt[k], std::max<int64_t>(256, (int64_t)(share / std::max(spq[k], 1e-9)))) : 0;
-  collect(want, smp);
-  double est = 0.0;
-  int64_t tot = 0;
-  int nout = 0;
-  for (int k = 0; k < nkey; ++k) {
-    if (!cnt[k]) continue;
-    const double sec = run(smp[k]);
-    est += sec / smp[k].size() * cnt[k];
-    tot += cnt[k];
-    if (nout < maxcls) {
-      int v = k;
-      for (int m = 3; m >= 0; --m) {
-        cls_l[4 * nout + m] = v % L1;
-        v /= L1;
-      }
-      cls_count[nout] = cnt[k];
-      cls_sample[nout] = (int64_t)smp[k].size();
-      cls_seconds[nout] = sec;
-    }
-    ++nout;
+#pragma omp critical
+    smp.insert(smp.end(), mine.begin(), mine.end());
   }
-  *ncls = nout;
-  *est_seconds = est;
-  *total = tot;
+  std::sort(smp.begin(), smp.end(), [](const std::pair<int, int> &x, const std::pair<int, int> &y) {
+    return x.first != y.first ? x.first > y.first : x.second < y.second;
+  });
+  int64_t nq = 0;
+  const double t0 = omp_get_wtime();
+#pragma omp parallel reduction(+ : nq)
+  {
+    std::vector<double> Fl(N2, 0.0);
+    const double keep = 1.0;
+    EriWork w;
+    std::vector<double> g, cart, tmp;
+#pragma omp for schedule(dynamic, 8)
+    for (int64_t i = 0; i < (int64_t)smp.size(); ++i) {
+      const int ab = smp[i].first, cd = smp[i].second;
+      const int sA = pairs[ab].first, sB = pairs[ab].second, sC = pairs[cd].first, sD = pairs[cd].second;
+      ++nq;
+      shell_eri(B, sA, sB, sC, sD, g, w, cart, tmp);
+      digest_quartet(B, sA, sB, sC, sD, ab == cd, g, ds, 1, 0.5, &keep, &keep, -1.0, Fl.data());
+    }
+  }
+  *seconds = omp_get_wtime() - t0;
+  *nsample = nq;
+  *total = ntot;
   return 0;
 }
 

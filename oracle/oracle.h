@@ -71,13 +71,12 @@ int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double 
 int orc_fock_screened(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
                       double hfxfac, double thrs, int64_t ifthrs, int64_t icedif, int64_t *counts);
 
-/* Class-stratified timing of a J+K build (IFCTYP 13, hfxfac 1) for the CPU
- * baseline: per class (lA lB|lC lD) of significant segmented quartets, a
- * count and a timed evenly spaced sample; *est_seconds is the extrapolated
- * time of the whole build (see oracle.cpp). */
-int orc_fock_class_sample(const orc_basis *b, const double *dmat, double thrs, double target_seconds, int maxcls,
-                          int64_t *cls_l, int64_t *cls_count, int64_t *cls_sample, double *cls_seconds, int *ncls,
-                          double *est_seconds, int64_t *total);
+/* Timing sample of a J+K build (IFCTYP 13, hfxfac 1) for the CPU baseline:
+ * the significant quartets whose hash falls in a fixed 2^-k fraction (the
+ * workload's class mix), evaluated and digested on all threads; *nsample
+ * quartets in *seconds, *total significant quartets (see oracle.cpp). */
+int orc_fock_hash_sample(const orc_basis *b, const double *dmat, double thrs, int k, int64_t *nsample,
+                         double *seconds, int64_t *total);
 
 /* Sampled J+K build (IFCTYP 13, hfxfac 1) over the bra pairs ab with
  * ab % stride == offset, for CPU-baseline timing; *nquartet = quartets done. */

@@ -56,9 +56,8 @@ def lib():
         _lib.orc_schwarz.argtypes = [ctypes.POINTER(OrcBasis), _dp, _i64p, _i64p, _i64p]
         _lib.orc_fock_screened.argtypes = [ctypes.POINTER(OrcBasis), ctypes.c_int, _i64p, _dp, _dp,
                                            ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _i64p]
-        _lib.orc_fock_class_sample.argtypes = [ctypes.POINTER(OrcBasis), _dp, ctypes.c_double, ctypes.c_double,
-                                               ctypes.c_int, _i64p, _i64p, _i64p, _dp,
-                                               ctypes.POINTER(ctypes.c_int), _dp, _i64p]
+        _lib.orc_fock_hash_sample.argtypes = [ctypes.POINTER(OrcBasis), _dp, ctypes.c_double, ctypes.c_int, _i64p,
+                                              _dp, _i64p]
     return _lib
 
 
@@ -160,26 +159,17 @@ def fock_screened(bs, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, icedif
     return (f[0] if single else f), counts
 
 
-def fock_class_sample(bs, dmat, thrs=1e-12, target_seconds=10.0):
-    """Class-stratified timing of the J+K build (see oracle.h): returns a dict
-    with the extrapolated seconds of the whole build, the quartet count and a
-    per-class table."""
+def fock_hash_sample(bs, dmat, k, thrs=1e-12):
+    """Timing sample of the J+K build (see oracle.h): a fixed pseudo-random
+    2^-k fraction of the significant quartets.  Returns (quartets evaluated,
+    seconds, significant quartets in all)."""
     h = _Holder(bs)
     d = np.ascontiguousarray(dmat, dtype=np.float64)
-    maxcls = 512
-    cl = np.zeros(4 * maxcls, dtype=np.int64)
-    cc, cs = np.zeros(maxcls, dtype=np.int64), np.zeros(maxcls, dtype=np.int64)
-    sec = np.zeros(maxcls)
-    n = ctypes.c_int()
-    est = ctypes.c_double()
-    tot = ctypes.c_int64()
-    lib().orc_fock_class_sample(ctypes.byref(h.s), _p(d, ctypes.c_double), float(thrs), float(target_seconds), maxcls,
-                                _p(cl, ctypes.c_int64), _p(cc, ctypes.c_int64), _p(cs, ctypes.c_int64),
-                                _p(sec, ctypes.c_double), ctypes.byref(n), ctypes.byref(est), ctypes.byref(tot))
-    k = min(n.value, maxcls)
-    classes = [{"class": [int(x) for x in cl[4 * i:4 * i + 4]], "count": int(cc[i]), "sample": int(cs[i]),
-                "sample_seconds": float(sec[i])} for i in range(k)]
-    return {"est_seconds": est.value, "quartets": int(tot.value), "classes": classes}
+    nq, tot = ctypes.c_int64(), ctypes.c_int64()
+    sec = ctypes.c_double()
+    lib().orc_fock_hash_sample(ctypes.byref(h.s), _p(d, ctypes.c_double), float(thrs), int(k), ctypes.byref(nq),
+                               ctypes.byref(sec), ctypes.byref(tot))
+    return nq.value, sec.value, tot.value
 
 
 def fock(bs, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12) -> np.ndarray:

@@ -67,14 +67,17 @@ def test_zero_density_blocks_are_skipped_exactly(orc):
     assert np.abs(f - ref).max() < 1e-13
 
 
-def test_class_sample_counts_every_quartet(orc):
-    """The stratified sampler counts exactly the significant quartets the
-    full build evaluates, and its class table adds up to that count."""
+def test_hash_sample_is_a_fixed_uniform_subset(orc):
+    """The CPU-baseline sample: k = 0 evaluates every significant quartet; a
+    2^-k sample holds about that fraction of them, the same subset every
+    time."""
     bs = _water_pair()
     d = _density(bs.nbf, 5)
-    r = orc.fock_class_sample(bs, d, 1e-12, 0.5)
+    n0, _, tot = orc.fock_hash_sample(bs, d, 0)
     _, nq = orc.fock_sampled(bs, d, 1, 0, 1e-12)
-    assert r["quartets"] == nq
-    assert sum(c["count"] for c in r["classes"]) == nq
-    assert all(0 < c["sample"] <= c["count"] for c in r["classes"])
-    assert r["est_seconds"] > 0.0
+    assert n0 == tot == nq
+    n4, s4, tot4 = orc.fock_hash_sample(bs, d, 4)
+    assert tot4 == tot
+    assert abs(n4 - tot / 16) < 5 * (tot / 16) ** 0.5
+    assert orc.fock_hash_sample(bs, d, 4)[0] == n4
+    assert s4 > 0.0
