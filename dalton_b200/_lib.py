@@ -35,7 +35,7 @@ class DgfBasis(ctypes.Structure):
 class DgfOptions(ctypes.Structure):
     _fields_ = [("thrs", ctypes.c_double), ("ifthrs", dgf_int), ("hfxfac", ctypes.c_double),
                 ("mixed_cutoff", ctypes.c_double), ("shard_index", dgf_int), ("shard_count", dgf_int),
-                ("icedif", dgf_int)]
+                ("icedif", dgf_int), ("hfxmu", ctypes.c_double), ("hfxatt", ctypes.c_double)]
 
 
 class DgfStats(ctypes.Structure):

@@ -611,6 +611,8 @@ extern "C" void dgf_default_options(dgf_options *opt) {
   opt->shard_index = 0;
   opt->shard_count = 1;
   opt->icedif = 3;
+  opt->hfxmu = 0.0;
+  opt->hfxatt = 0.0;
 }
 
 extern "C" int dgf_create(const dgf_basis *b, int device, dgf_ctx **out) {
@@ -1067,7 +1069,8 @@ static int ensure_block_screen(dgf_ctx *c, int nslot) {
 
 struct SlotSpec {
   int src, op;
-  double js, ks;
+  double js, ks;  // Coulomb and exchange scales of the 1/r12 pass
+  double ka;      // exchange scale of the attenuated erf(mu r12)/r12 pass
 };
 
 // Model cost of one quartet of a plan entry: the fixed FLOP model of the
@@ -1141,6 +1144,8 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     bool zero;
   };
   std::vector<OutSpec> outs;
+  if (!std::isfinite(o.hfxmu) || !std::isfinite(o.hfxatt)) DGF_FAIL(DGF_ERR_ARG, "hfxmu and hfxatt must be finite");
+  const bool attenuated = o.hfxmu != 0.0 && o.hfxatt != 0.0;
   for (int k = 0; k < ndmat; ++k) {
     const int X = (int)(ifctyp[k] / 10), Y0 = (int)(ifctyp[k] % 10);
     if (X < 0 || X > 2 || Y0 < 1 || Y0 > 3) DGF_FAIL(DGF_ERR_UNSUPPORTED, "unsupported IFCTYP");
@@ -1148,21 +1153,23 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     if (X == 2) Y &= 2;                 // antisymmetric density: no Coulomb part
     if (o.hfxfac == 0.0) Y &= 1;        // no exchange
     const double js = (Y & 1) ? 1.0 : 0.0, ks = (Y & 2) ? 0.5 * o.hfxfac : 0.0;
-    if (Y == 0) {
+    // attenuated pass: exchange only, scaled by HFXATT (herfckcon.F:59-66)
+    const double ka = attenuated ? 0.5 * o.hfxatt : 0.0;
+    if (Y == 0 && ka == 0.0) {
       outs.push_back({0, 0, 0.0, true});
       continue;
     }
     if (X == 1) {
-      slots.push_back({k, 2, js, ks});
+      slots.push_back({k, 2, js, ks, ka});
       const int s = (int)slots.size() - 1;
       outs.push_back({s, s, 1.0, false});
     } else if (X == 2) {
-      slots.push_back({k, 3, js, ks});
+      slots.push_back({k, 3, js, ks, ka});
       const int s = (int)slots.size() - 1;
       outs.push_back({s, s, -1.0, false});
     } else {
-      slots.push_back({k, 0, js, ks});
-      slots.push_back({k, 1, js, ks});
+      slots.push_back({k, 0, js, ks, ka});
+      slots.push_back({k, 1, js, ks, ka});
       const int s = (int)slots.size() - 2;
       outs.push_back({s, s + 1, 1.0, false});
     }
@@ -1230,10 +1237,6 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     a.D = c->d_D;
     a.Ds = c->d_Ds;
     a.Fh = c->d_Fh;
-    for (int s = 0; s < ns; ++s) {
-      a.jscale[s] = slots[s0 + s].js;
-      a.kscale[s] = slots[s0 + s].ks;
-    }
     a.dmax = need_dmax ? c->d_dmax : nullptr;
     a.dens_thr = doscrn ? std::pow(10.0, -(double)ifthrs) : 0.0;
     a.blk_gab = doscrn ? c->d_blk_gab : nullptr;
@@ -1246,37 +1249,49 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
     a.split = o.mixed_cutoff;
     a.schwarz_thr = o.thrs;
     a.mode = 0;
-    for (size_t e = 0; e < c->plan.size(); ++e) {
-      const ClassPlan &cp = c->plan[e];
-      if (sq1[e] <= sq0[e]) continue;  // not in this shard
-      a.bra = c->d_pairs + c->cls_off[cp.X];
-      a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
-      a.ket_off = cp.kb0;
-      a.ket_pp0 = ket_pp0_of(c, cp);
-      set_ket_table(c, cp, a);
-      a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
-      a.same_class = (cp.X == cp.Y);
-      a.qoff = c->d_qoff + cp.off;
-      a.q_begin = sq0[e];
-      a.nquartet = sq1[e];
-      // Boys table of order L = la+lb+lc+ld.
-      const int la = (cp.X == 0) ? 0 : (cp.X <= 2) ? 1 : (cp.X <= 5) ? 2 : 3;
-      const int lb = cp.X - la * (la + 1) / 2;
-      const int lc = (cp.Y == 0) ? 0 : (cp.Y <= 2) ? 1 : (cp.Y <= 5) ? 2 : 3;
-      const int ld = cp.Y - lc * (lc + 1) / 2;
-      a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-      const bool split = o.mixed_cutoff > 0.0 && c->split_ok[cp.X][cp.Y] &&
-                         select_kernel(c, cp.X, cp.Y, 1, cp.bucket == 0).launch != nullptr;
-      const int Lq = la + lb + lc + ld;
-      for (int part = 0; part < (split ? 2 : 1); ++part) {
-        a.mode = split ? 1 + part : 0;
-        // the FP32 half reads the low-degree Boys table
-        a.boys = c->d_boys + ((split && part == 1) ? boys_low_offset(Lq) : (size_t)Lq * kBoysTableDoubles);
-        a.counters = c->d_cnt + 4 * (nlaunch_class % kCounterSlots);
-        ++nlaunch_class;
-        int r = launch_class(c, cp.X, cp.Y, a, st, split && part == 1 ? 1 : 0, cp.bucket == 0);
-        if (r) return r;
-        ++launches;
+    // Pass 0: 1/r12 with the slots' Coulomb and exchange scales; pass 1
+    // (range-separated exchange): erf(mu r12)/r12, exchange only.
+    for (int pass = 0; pass < (attenuated ? 2 : 1); ++pass) {
+      bool any = false;
+      for (int s = 0; s < ns; ++s) {
+        a.jscale[s] = pass == 0 ? slots[s0 + s].js : 0.0;
+        a.kscale[s] = pass == 0 ? slots[s0 + s].ks : slots[s0 + s].ka;
+        any = any || a.jscale[s] != 0.0 || a.kscale[s] != 0.0;
+      }
+      a.erf_mu2 = pass == 0 ? 0.0 : o.hfxmu * o.hfxmu;
+      if (!any) continue;
+      for (size_t e = 0; e < c->plan.size(); ++e) {
+        const ClassPlan &cp = c->plan[e];
+        if (sq1[e] <= sq0[e]) continue;  // not in this shard
+        a.bra = c->d_pairs + c->cls_off[cp.X];
+        a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
+        a.ket_off = cp.kb0;
+        a.ket_pp0 = ket_pp0_of(c, cp);
+        set_ket_table(c, cp, a);
+        a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
+        a.same_class = (cp.X == cp.Y);
+        a.qoff = c->d_qoff + cp.off;
+        a.q_begin = sq0[e];
+        a.nquartet = sq1[e];
+        // Boys table of order L = la+lb+lc+ld.
+        const int la = (cp.X == 0) ? 0 : (cp.X <= 2) ? 1 : (cp.X <= 5) ? 2 : 3;
+        const int lb = cp.X - la * (la + 1) / 2;
+        const int lc = (cp.Y == 0) ? 0 : (cp.Y <= 2) ? 1 : (cp.Y <= 5) ? 2 : 3;
+        const int ld = cp.Y - lc * (lc + 1) / 2;
+        a.boys = c->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
+        const bool split = o.mixed_cutoff > 0.0 && c->split_ok[cp.X][cp.Y] &&
+                           select_kernel(c, cp.X, cp.Y, 1, cp.bucket == 0).launch != nullptr;
+        const int Lq = la + lb + lc + ld;
+        for (int part = 0; part < (split ? 2 : 1); ++part) {
+          a.mode = split ? 1 + part : 0;
+          // the FP32 half reads the low-degree Boys table
+          a.boys = c->d_boys + ((split && part == 1) ? boys_low_offset(Lq) : (size_t)Lq * kBoysTableDoubles);
+          a.counters = c->d_cnt + 4 * (nlaunch_class % kCounterSlots);
+          ++nlaunch_class;
+          int r = launch_class(c, cp.X, cp.Y, a, st, split && part == 1 ? 1 : 0, cp.bucket == 0);
+          if (r) return r;
+          ++launches;
+        }
       }
     }
     // Combine the slots of this chunk into the outputs they belong to.

@@ -378,8 +378,8 @@ extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, do
   dgf_options o;
   dgf_default_options(&o);
   if (opt) o = *opt;
-  if (o.ifthrs < 16 || o.mixed_cutoff > 0.0 || o.shard_count > 1)
-    BFAIL(DGF_ERR_UNSUPPORTED, "batched builds take the FP64 Schwarz-screened form only");
+  if (o.ifthrs < 16 || o.mixed_cutoff > 0.0 || o.shard_count > 1 || o.hfxmu != 0.0)
+    BFAIL(DGF_ERR_UNSUPPORTED, "batched builds take the Schwarz-screened form without range separation only");
   cudaStream_t st = (cudaStream_t)stream;  // NULL: the legacy default stream, as in dgf_fock_device
   int r = batch_plan(b, o.thrs);
   if (r) return r;

@@ -119,6 +119,7 @@ struct JKArgs {
   double dens_thr;          // skip if bound < dens_thr (0: no density screening)
   double split;             // precision split bound
   double schwarz_thr;       // skip quartets with Q_AB Q_CD below this (0: the plan is exact)
+  double erf_mu2;           // > 0: the attenuated operator erf(mu r12)/r12 with mu^2 = erf_mu2; 0: 1/r12
   int mode;                 // 0: all, 1: bound >= split only, 2: bound < split only
   double *diag_out;         // Schwarz mode: sqrt(max |(ab|ab)|) per bra pair, no digestion
   unsigned long long *counters;  // [0] quartets done, [1] primitive quartets, [2] skipped

@@ -159,11 +159,12 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
         if (tid == (nt > 32 ? 32 : 3)) {
           const double p = P1.p, qq = P2.p;
           const double rs = rsqrt(p + qq);
-          const double alpha = p * qq * rs * rs;
+          double alpha = p * qq * rs * rs;
+          double s = P1.K * P2.K * rs;
+          erf_attenuate(a.erf_mu2, alpha, s);
           const double x = P1.Px - P2.Px, y = P1.Py - P2.Py, z = P1.Pz - P2.Pz;
           double F[L + 1];
           boys_eval<L>(alpha * (x * x + y * y + z * z), tab, F);
-          double s = P1.K * P2.K * rs;
           for (int n = 0; n <= L; ++n) {
             sF[n] = s * F[n];
             s *= -2.0 * alpha;

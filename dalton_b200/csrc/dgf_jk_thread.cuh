@@ -348,12 +348,13 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
         auto ket_prim = [&](const PrimPair &P2) {
           // FP32 half: FP32 rsqrt for the prefactor and the low-degree FP64 Boys table
           const double rs = (sizeof(Tc) == 4) ? (double)rsqrtf((float)(P1.p + P2.p)) : rsqrt(P1.p + P2.p);
-          const double alpha = P1.p * P2.p * rs * rs;
+          double alpha = P1.p * P2.p * rs * rs;
+          double s = P1.K * P2.K * rs;
+          erf_attenuate(a.erf_mu2, alpha, s);
           const double x = P1.Px - P2.Px, y = P1.Py - P2.Py, z = P1.Pz - P2.Pz;
           double F[L + 1];
           boys_eval<L, (sizeof(Tc) == 4) ? kBoysDegLow : kBoysDeg>(alpha * (x * x + y * y + z * z), tab, F);
           Tc Fs[L + 1];
-          double s = P1.K * P2.K * rs;
 #pragma unroll
           for (int n = 0; n <= L; ++n) {
             Fs[n] = Tc(s * F[n]);

@@ -429,13 +429,14 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
         }
         // Boys function and scaled R^n_000 (every lane, the same values)
         const double rs = (sizeof(Tc) == 4) ? (double)rsqrtf((float)(P1.p + P2.p)) : rsqrt(P1.p + P2.p);
-        const double alpha = P1.p * P2.p * rs * rs;
+        double alpha = P1.p * P2.p * rs * rs;
+        double s = P1.K * P2.K * rs;
+        erf_attenuate(a.erf_mu2, alpha, s);
         const double x = P1.Px - P2.Px, y = P1.Py - P2.Py, z = P1.Pz - P2.Pz;
         double F[L + 1];
         boys_eval<L, (sizeof(Tc) == 4) ? kBoysDegLow : kBoysDeg>(alpha * (x * x + y * y + z * z), tab, F);
         double Fs[L + 1];
         {
-          double s = P1.K * P2.K * rs;
 #pragma unroll
           for (int n = 0; n <= L; ++n) {
             Fs[n] = s * F[n];

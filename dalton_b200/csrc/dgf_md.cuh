@@ -82,6 +82,19 @@ __device__ __forceinline__ void boys_eval(double T, const double *__restrict__ t
   }
 }
 
+// The attenuated Coulomb operator erf(mu r12)/r12 of range-separated
+// exchange (Dalton's HFXMU pass, DALTON/abacus/her2her.F:344-353): with
+// beta = mu^2 / (alpha + mu^2), R^n_000 takes alpha * beta in place of alpha,
+// in the Boys argument and in (-2 alpha)^n, and its prefactor gains
+// sqrt(beta).  mu2 = 0 leaves the plain 1/r12 operator.
+__device__ __forceinline__ void erf_attenuate(double mu2, double &alpha, double &pref) {
+  if (mu2 > 0.0) {
+    const double beta = mu2 / (alpha + mu2);
+    alpha *= beta;
+    pref *= sqrt(beta);
+  }
+}
+
 // Hermite expansion coefficients of one direction, E^{ij}_t for i <= LA,
 // j <= LB, t <= i+j, E^{00}_0 = 1; layout E[(i*(LB+1)+j)*(LA+LB+1)+t].
 // h = 1/(2p).  SIGN = -1 multiplies E_t by (-1)^t (ket side of the MD sum).

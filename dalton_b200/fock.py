@@ -83,10 +83,12 @@ class FockBuilder:
         return np.ascontiguousarray(np.broadcast_to(np.asarray(ifctyp, dtype=np.int64), (nd,)))
 
     def herfck(self, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, mixed_cutoff=0.0, shard=(0, 1),
-               icedif=3) -> np.ndarray:
+               icedif=3, hfxmu=0.0, hfxatt=0.0) -> np.ndarray:
         """F = [Y&1] J[D] - [Y&2] hfxfac/2 K[D] for host matrices (N,N) or (ndmat,N,N).
         Density screening (Dalton's .IFTHRS) is on for ifthrs < 16, with
-        Dalton's separate Coulomb/exchange skips per ``icedif`` (.ICEDIF)."""
+        Dalton's separate Coulomb/exchange skips per ``icedif`` (.ICEDIF).
+        With ``hfxmu`` != 0 (range-separated hybrids) F also gets
+        -hfxatt/2 K[D] of the operator erf(hfxmu r12)/r12."""
         d = np.ascontiguousarray(dmat, dtype=np.float64)
         single = d.ndim == 2
         if single:
@@ -98,7 +100,8 @@ class FockBuilder:
         f = np.empty_like(d)
         opt = _lib.default_options(thrs=float(thrs), ifthrs=int(ifthrs), hfxfac=float(hfxfac),
                                    mixed_cutoff=float(mixed_cutoff), shard_index=int(shard[0]),
-                                   shard_count=int(shard[1]), icedif=int(icedif))
+                                   shard_count=int(shard[1]), icedif=int(icedif), hfxmu=float(hfxmu),
+                                   hfxatt=float(hfxatt))
         st = _lib.DgfStats()
         _lib.check(self._lib.dgf_fock(self._h, nd, ift.ctypes.data_as(ctypes.POINTER(_lib.dgf_int)), _dp(d), _dp(f),
                                       ctypes.byref(opt), ctypes.byref(st)), "dgf_fock")
@@ -106,7 +109,7 @@ class FockBuilder:
         return f[0] if single else f
 
     def herfck_device(self, dmat, fmat=None, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, mixed_cutoff=0.0,
-                      stream=None, stats=True, shard=(0, 1), icedif=3):
+                      stream=None, stats=True, shard=(0, 1), icedif=3, hfxmu=0.0, hfxatt=0.0):
         """Device form: ``dmat`` a CUDA float64 tensor (N,N) or (ndmat,N,N)."""
         import torch
 
@@ -119,7 +122,8 @@ class FockBuilder:
         ift = self._ifctyp(ifctyp, nd)
         opt = _lib.default_options(thrs=float(thrs), ifthrs=int(ifthrs), hfxfac=float(hfxfac),
                                    mixed_cutoff=float(mixed_cutoff), shard_index=int(shard[0]),
-                                   shard_count=int(shard[1]), icedif=int(icedif))
+                                   shard_count=int(shard[1]), icedif=int(icedif), hfxmu=float(hfxmu),
+                                   hfxatt=float(hfxatt))
         if stream is None:
             stream = torch.cuda.current_stream(d.device).cuda_stream
         st = _lib.DgfStats()

@@ -113,13 +113,24 @@ typedef struct {
    * density when max|D| over its Coulomb blocks times the quartet's largest
    * integral is below 10^-ifthrs, bit 2 likewise its exchange contribution
    * (INTFC1, DALTON/abacus/her2fck.F:221-222,446-466).  Dalton's default is
-   * 3.  The thread-per-quartet kernels apply it; quartets of the cooperative
-   * kernels are always digested whole (the conservative side). */
+   * 3.  The thread- and warp-per-quartet kernels apply it; quartets of the
+   * cooperative kernels are always digested whole (the conservative side). */
   dgf_int icedif;
+  /* Range-separated exchange of CAM-type functionals (Dalton's HFXMU and
+   * HFXATT, set by dftsetcam, DALTON/dft/dft_aux.F:346-351): with hfxmu != 0
+   * a second pass over the quartets adds -hfxatt/2 K[D] computed with the
+   * attenuated operator erf(hfxmu r12)/r12, exchange only whatever the
+   * Coulomb digit of IFCTYP (HERFCK_1, DALTON/abacus/herdirect.F:792-835;
+   * FCKCON forces IY = 2, herfckcon.F:59-66; attenuated R^n_000,
+   * her2her.F:344-353).  The Schwarz factors of 1/r12 bound the attenuated
+   * integrals too (erf(mu r)/r <= 1/r, positive definite), so the same
+   * quartet plan serves both passes.  hfxmu = 0: no second pass. */
+  double hfxmu;
+  double hfxatt;
 } dgf_options;
 
 /* Default options: thrs 1e-12, ifthrs 20, hfxfac 1, mixed_cutoff 0, one
- * shard, icedif 3. */
+ * shard, icedif 3, hfxmu 0, hfxatt 0. */
 void dgf_default_options(dgf_options *opt);
 
 /* Create a context on CUDA device `device`: copies the basis to the device,

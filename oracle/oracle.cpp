@@ -263,6 +263,9 @@ Basis make_basis(const orc_basis *b) {
 struct EriWork {
   std::vector<double> ex1, ey1, ez1, ex2, ey2, ez2, R, X;
   RWork rw;
+  // > 0: the attenuated operator erf(mu r12)/r12 with mu^2 = mu2 (HFXMU
+  // branch of R0001, DALTON/abacus/her2her.F:344-353); 0: 1/r12.
+  double mu2 = 0.0;
 };
 void prim_eri(int la, int lb, int lc, int ld, double a, double b, double c, double d, const double *A,
               const double *Bc, const double *C, const double *D, double scale, double *out, EriWork &w) {
@@ -280,6 +283,11 @@ void prim_eri(int la, int lb, int lc, int ld, double a, double b, double c, doub
   double kab = std::exp(-a * b / p * ab2), kcd = std::exp(-c * d / q * cd2);
   double alpha = p * q / (p + q);
   double pref = 2.0 * std::pow(kPi, 2.5) / (p * q * std::sqrt(p + q)) * kab * kcd * scale;
+  if (w.mu2 > 0.0) {  // BETA = HFXMU^2 / (ALPHA + HFXMU^2): alpha -> alpha*beta, prefactor * sqrt(beta)
+    const double beta = w.mu2 / (alpha + w.mu2);
+    alpha *= beta;
+    pref *= std::sqrt(beta);
+  }
   hermite_e(la, lb, p, P[0] - A[0], P[0] - Bc[0], w.ex1);
   hermite_e(la, lb, p, P[1] - A[1], P[1] - Bc[1], w.ey1);
   hermite_e(la, lb, p, P[2] - A[2], P[2] - Bc[2], w.ez1);
@@ -505,6 +513,11 @@ struct FockOpts {
   double hfxfac = 1.0, thrs = 1e-12;
   int ifthrs = 20, icedif = 3;
   int stride = 1, offset = 0;
+  // attenuated pass of HERFCK_1 (DALTON/abacus/herdirect.F:815-835): the
+  // operator erf(mu r12)/r12 (mu2 = HFXMU^2) and exchange only for every
+  // density (FCKCON sets IY = 2, herfckcon.F:66), hfxfac = HFXATT.
+  double mu2 = 0.0;
+  bool exchange_only = false;
 };
 
 struct FockCounts {
@@ -570,6 +583,40 @@ int orc_fock_screened(const orc_basis *b, int ndmat, const int64_t *ifctyp, cons
     counts[4] = c.dropped_k;
   }
   return r;
+}
+
+// HERFCK_1 with range-separated exchange (DALTON/abacus/herdirect.F:792-835):
+// the 1/r12 build with HFXFAC, then, when HFXMU != 0, a second TWOINT pass
+// with the operator erf(HFXMU r12)/r12, HFXFAC replaced by HFXATT and only
+// the exchange part of every density, added to the same FMAT.
+int orc_fock_attenuated(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
+                        double hfxfac, double thrs, double hfxmu, double hfxatt) {
+  FockOpts o;
+  o.hfxfac = hfxfac;
+  o.thrs = thrs;
+  int r = fock_core(b, ndmat, ifctyp, dmat, fmat, o, nullptr);
+  if (r || hfxmu == 0.0) return r;
+  const size_t n2 = (size_t)ndmat * b->nbf * b->nbf;
+  std::vector<double> f2(n2);
+  FockOpts o2;
+  o2.hfxfac = hfxatt;
+  o2.thrs = thrs;
+  o2.mu2 = hfxmu * hfxmu;
+  o2.exchange_only = true;
+  r = fock_core(b, ndmat, ifctyp, dmat, f2.data(), o2, nullptr);
+  for (size_t i = 0; i < n2; ++i) fmat[i] += f2[i];
+  return r;
+}
+
+// One primitive (la lb|lc ld) Cartesian block with the operator erf(mu r12)/r12
+// (mu = 0: 1/r12), out[((a*nb+b)*nc+c)*nd+d]; for tests of the attenuation.
+void orc_prim_eri(int la, int lb, int lc, int ld, const double *exps, const double *centers, double mu, double *out) {
+  EriWork w;
+  w.mu2 = mu * mu;
+  const size_t n = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+  for (size_t i = 0; i < n; ++i) out[i] = 0.0;
+  prim_eri(la, lb, lc, ld, exps[0], exps[1], exps[2], exps[3], centers, centers + 3, centers + 6, centers + 9, 1.0,
+           out, w);
 }
 
 int orc_fock_sampled(const orc_basis *b, const double *dmat, double *fmat, double thrs, int stride, int offset,
@@ -696,7 +743,12 @@ static int fock_core(const orc_basis *b, int ndmat, const int64_t *ifctyp, const
   Basis B = make_basis(b);
   int ns = (int)B.sh.size();
   size_t N = B.nbf, N2 = N * N;
-  const DensitySet ds = decode_densities(N, ndmat, ifctyp, dmat, o.hfxfac);
+  DensitySet ds = decode_densities(N, ndmat, ifctyp, dmat, o.hfxfac);
+  if (o.exchange_only)
+    for (int k = 0; k < ndmat; ++k) {
+      ds.doJ[k] = 0;
+      ds.doK[k] = o.hfxfac != 0.0;
+    }
   std::vector<double> Q = schwarz(B);
   const BlockBounds bb = block_bounds(B, Q, ds.D.data(), ndmat);
   int ifthrs = o.ifthrs;
@@ -715,6 +767,7 @@ static int fock_core(const orc_basis *b, int ndmat, const int64_t *ifctyp, const
     std::vector<double> Fl(ndmat * N2, 0.0);
     std::vector<double> dJ(ndmat), dK(ndmat), jkeep(ndmat), kkeep(ndmat);
     EriWork w;
+    w.mu2 = o.mu2;
     std::vector<double> g, cart, tmp;
 #pragma omp for schedule(dynamic)
     for (int ab = npair - 1; ab >= 0; --ab) {

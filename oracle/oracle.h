@@ -71,6 +71,18 @@ int orc_fock(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double 
 int orc_fock_screened(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
                       double hfxfac, double thrs, int64_t ifthrs, int64_t icedif, int64_t *counts);
 
+/* HERFCK_1 with range-separated exchange (DALTON/abacus/herdirect.F:792-835):
+ * orc_fock, then for hfxmu != 0 a second pass with the operator
+ * erf(hfxmu r12)/r12 adding -hfxatt/2 K[D] (exchange only for every
+ * density, FCKCON's IY = 2 of herfckcon.F:66). */
+int orc_fock_attenuated(const orc_basis *b, int ndmat, const int64_t *ifctyp, const double *dmat, double *fmat,
+                        double hfxfac, double thrs, double hfxmu, double hfxatt);
+
+/* One primitive Cartesian block (la lb|lc ld) of unnormalised Gaussians with
+ * exponents exps[4] at centers[4][3], operator erf(mu r12)/r12 (mu = 0:
+ * 1/r12), out[((a*nb+b)*nc+c)*nd+d]. */
+void orc_prim_eri(int la, int lb, int lc, int ld, const double *exps, const double *centers, double mu, double *out);
+
 /* Timing sample of a J+K build (IFCTYP 13, hfxfac 1) for the CPU baseline:
  * the significant quartets whose hash falls in a fixed 2^-k fraction (the
  * workload's class mix), evaluated and digested on all threads; *nsample

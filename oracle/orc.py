@@ -58,6 +58,11 @@ def lib():
                                            ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _i64p]
         _lib.orc_fock_hash_sample.argtypes = [ctypes.POINTER(OrcBasis), _dp, ctypes.c_double, ctypes.c_int, _i64p,
                                               _dp, _i64p]
+        _lib.orc_fock_attenuated.argtypes = [ctypes.POINTER(OrcBasis), ctypes.c_int, _i64p, _dp, _dp,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        _lib.orc_prim_eri.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                      ctypes.c_double, _dp]
+        _lib.orc_prim_eri.restype = None
     return _lib
 
 
@@ -157,6 +162,35 @@ def fock_screened(bs, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, icedif
     counts = dict(zip(("evaluated", "skipped_screen", "skipped_zero", "dropped_coulomb", "dropped_exchange"),
                       (int(x) for x in c)))
     return (f[0] if single else f), counts
+
+
+def fock_attenuated(bs, dmat, ifctyp=13, hfxfac=1.0, thrs=1e-12, hfxmu=0.0, hfxatt=0.0):
+    """HERFCK with range-separated exchange: the 1/r12 build plus, for
+    hfxmu != 0, -hfxatt/2 K[D] of erf(hfxmu r12)/r12 (see oracle.h)."""
+    h = _Holder(bs)
+    d = np.ascontiguousarray(dmat, dtype=np.float64)
+    single = d.ndim == 2
+    if single:
+        d = d[None]
+    nd = d.shape[0]
+    ift = np.ascontiguousarray(np.broadcast_to(np.asarray(ifctyp, dtype=np.int64), (nd,)))
+    f = np.zeros_like(d)
+    lib().orc_fock_attenuated(ctypes.byref(h.s), nd, _p(ift, ctypes.c_int64), _p(d, ctypes.c_double),
+                              _p(f, ctypes.c_double), float(hfxfac), float(thrs), float(hfxmu), float(hfxatt))
+    return f[0] if single else f
+
+
+def prim_eri(ls, exps, centers, mu=0.0):
+    """One primitive Cartesian (la lb|lc ld) block of unnormalised Gaussians
+    with the operator erf(mu r12)/r12 (mu = 0: 1/r12); shape (na, nb, nc, nd)."""
+    ls = [int(x) for x in ls]
+    nc = [(x + 1) * (x + 2) // 2 for x in ls]
+    e = np.ascontiguousarray(exps, dtype=np.float64)
+    c = np.ascontiguousarray(centers, dtype=np.float64).reshape(12)
+    out = np.zeros(int(np.prod(nc)))
+    lib().orc_prim_eri(ls[0], ls[1], ls[2], ls[3], _p(e, ctypes.c_double), _p(c, ctypes.c_double), float(mu),
+                       _p(out, ctypes.c_double))
+    return out.reshape(nc)
 
 
 def fock_hash_sample(bs, dmat, k, thrs=1e-12):

@@ -68,3 +68,39 @@ def test_noalloc_rejects_oversized_and_unplanned(cuda):
     d = _density(small.nbf, 3, cuda)
     f = torch.empty_like(d)
     assert _noalloc(small, d, f, thrs=1e-12) == _lib.DGF_ERR_ARG  # no plan for this threshold yet
+
+
+@pytest.mark.parametrize("hfxfac", [1.0, 0.25, 0.0])
+def test_noalloc_hfxfac(cuda, hfxfac):
+    """The exchange scale: full exchange, a hybrid fraction and J only, each
+    against the regular device build with the same HFXFAC."""
+    import torch
+
+    bs = build_basis(molecules.water_cluster(2, seed=4), "cc-pVDZ")
+    fb = FockBuilder(bs)
+    d = _density(bs.nbf, 41, cuda)
+    ref = fb.herfck_device(d, hfxfac=hfxfac).clone()
+    out = torch.full_like(d, float("nan"))
+    assert _noalloc(fb, d, out, hfxfac=hfxfac) == _lib.DGF_OK, _lib.last_error()
+    torch.cuda.synchronize()
+    assert float(torch.max(torch.abs(out - ref))) < TOL
+
+
+@pytest.mark.parametrize("planner", ["autotune", "grad2e"])
+def test_noalloc_uses_plan_of_autotune_or_gradient(cuda, planner):
+    """A quartet plan made by the autotuner or by the gradient (not by a Fock
+    build) serves the no-allocation call; the autotuner's kernel choices apply."""
+    import torch
+
+    bs = build_basis(molecules.water_cluster(2, seed=6), "cc-pVDZ")
+    fb = FockBuilder(bs)
+    d = _density(bs.nbf, 43, cuda)
+    if planner == "autotune":
+        fb.autotune(d)
+    else:
+        fb.grad2e(d.cpu().numpy())
+    out = torch.full_like(d, float("nan"))
+    assert _noalloc(fb, d, out) == _lib.DGF_OK, _lib.last_error()
+    torch.cuda.synchronize()
+    ref = fb.herfck_device(d)
+    assert float(torch.max(torch.abs(out - ref))) < TOL
