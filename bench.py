@@ -33,7 +33,16 @@ METRIC = "J+K build ms & ERI quartets/s, mixed vs FP64 at <=1e-6 Eh; HF gradient
 MIXED_CUTOFF = 1e-6
 THRS = 1e-12
 # dgf_class_time.kernel: 0 thread-per-quartet, 1 cooperative team, 2 warp teams, 4 warp-per-quartet
-KERNEL_KIND = {0: "thread", 1: "team", 2: "team", 4: "warp"}
+KERNEL_KIND = {0: "thread", 1: "team", 2: "team", 4: "warp", 6: "warp"}
+
+
+def kernel_name(kind, la, lb, lc, ld, precision):
+    """Template name of a profiled class kernel (kind as dgf_class_time.kernel;
+    the warp kernel's last argument says whether its transforms run on the
+    FP64 tensor cores)."""
+    t = "double" if precision == 64 else "float"
+    mma = {4: ",false", 6: ",true"}.get(kind, "")
+    return f"jk_{KERNEL_KIND[kind]}_kernel<{la},{lb},{lc},{ld},{t}{mma}>"
 
 
 def parse():
@@ -53,6 +62,9 @@ def parse():
                     help="only run warmup+steps builds of a core-guess density (for ncu captures)")
     ap.add_argument("--mixed", action="store_true", help="with --profile-run: mixed form")
     ap.add_argument("--grad", action="store_true", help="with --profile-run: the two-electron gradient kernels")
+    ap.add_argument("--pin", action="append", default=[],
+                    help="with --profile-run: la,lb,lc,ld:variant pins one class's kernel (e.g. 2,1,2,1:-4 for the "
+                         "warp kernel with tensor-core transforms); repeatable")
     return ap.parse_args()
 
 
@@ -67,6 +79,9 @@ def profile_run(args):
     mol, basis = molecules.config(args.workload)
     bs = build_basis(mol, basis)
     fb = FockBuilder(bs)
+    for pin in args.pin:
+        cls, variant = pin.split(":")
+        fb.set_class_kernel(tuple(int(x) for x in cls.split(",")), int(variant))
     S, T, V = fb.oneint()
     Hm = torch.tensor(T + V, device="cuda")
     Sm = torch.tensor(S, device="cuda")
@@ -303,7 +318,7 @@ def batch_leg(workload, steps, warmup):
     # tune the kernel choices on the largest molecule and share them (loop and batch alike)
     big = max(range(len(fbs)), key=lambda k: fbs[k].nbf)
     t0 = time.perf_counter()
-    fbs[big].autotune(ds[big], thrs=THRS)
+    fbs[big].autotune(ds[big], thrs=THRS, mixed_cutoff=MIXED_CUTOFF)
     tune_s = time.perf_counter() - t0
     for fb in fbs:
         fb.copy_tuning_from(fbs[big])
@@ -336,6 +351,13 @@ def batch_leg(workload, steps, warmup):
     loop()
     torch.cuda.synchronize(dev)
     err = max(float(torch.max(torch.abs(a - b))) for a, b in zip(bb.unpack(fp), outs))
+    # mixed form of the batch (the split classes of the tuned context)
+    fpm = torch.empty_like(dp)
+    mixed_ms = timed(lambda: bb.herfck_batch(dp, fpm, use_graph=True, stats=False, mixed_cutoff=MIXED_CUTOFF))
+    bb.herfck_batch(dp, fpm, use_graph=True, mixed_cutoff=MIXED_CUTOFF)
+    stm = bb.last_stats
+    err_m = max(float(torch.max(torch.abs(a - b))) for a, b in zip(bb.unpack(fpm), outs))
+    de_m = max(abs(0.5 * float(torch.sum(d * (a - b)))) for d, a, b in zip(ds, bb.unpack(fpm), outs))
     for fb in fbs:
         fb.close()
     return {"workload": f"{workload}: {len(mols)} water clusters of 1-16 molecules (seeded), {basis}, "
@@ -343,7 +365,10 @@ def batch_leg(workload, steps, warmup):
             "quartets": st["quartets_total"], "steps": steps, "warmup": warmup,
             "per_molecule_loop_ms": loop_ms, "batched_graph_ms": graph_ms, "batched_no_graph_ms": nograph_ms,
             "speedup_graph_vs_loop": loop_ms / graph_ms, "quartets_per_s_graph": st["quartets_total"] / (graph_ms * 1e-3),
-            "launches_batched": st["kernel_launches"], "max_abs_diff_vs_loop": err, "context_setup_s": setup_s,
+            "launches_batched": st["kernel_launches"], "max_abs_diff_vs_loop": err,
+            "batched_graph_mixed_ms": mixed_ms, "mixed_fp32_quartets": stm["quartets_fp32"],
+            "mixed_max_abs_dF_vs_fp64": err_m, "mixed_max_energy_error_Eh": de_m,
+            "streams": 4, "context_setup_s": setup_s,
             "autotune_s_largest_molecule": tune_s,
             "data": "synthetic (seeded clusters, guess-like densities)"}
 
@@ -406,8 +431,7 @@ def top_kernel(fb, D, mixed_cutoff, fp64_peak, fp32_peak):
     peak = fp64_peak if k[4] == 64 else fp32_peak
     ach = flops / (a["ms"] * 1e-3) / 1e12
     tot = sum(v["ms"] for v in agg.values())
-    return {"kernel": f"jk_{KERNEL_KIND[k[5]]}_kernel<{k[0]},{k[1]},{k[2]},{k[3]},"
-                      f"{'double' if k[4] == 64 else 'float'}>", "ms": a["ms"], "quartets": a["evaluated"],
+    return {"kernel": kernel_name(k[5], k[0], k[1], k[2], k[3], k[4]), "ms": a["ms"], "quartets": a["evaluated"],
             "achieved_tflops": ach, "peak_tflops": peak, "frac": ach / peak, "share_of_build": a["ms"] / tot}
 
 
@@ -650,8 +674,7 @@ def main():
     achieved = top_flops / (top["ms"] * 1e-3) / 1e12
     peak = fp64_peak if top["precision"] == 64 else fp32_peak
     tot_ms = sum(r["ms"] for r in prof)
-    kname = lambda r: (f"jk_{KERNEL_KIND[r['kernel']]}_kernel<{r['la']},{r['lb']},{r['lc']},{r['ld']},"
-                       f"{'double' if r['precision'] == 64 else 'float'}>")
+    kname = lambda r: kernel_name(r["kernel"], r["la"], r["lb"], r["lc"], r["ld"], r["precision"])
     roofline = {"bound": "fp64" if top["precision"] == 64 else "fp32",
                 "kernel": kname(top),
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,

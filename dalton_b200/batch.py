@@ -51,13 +51,15 @@ class BatchBuilder:
         return [packed[self.offsets[k]:self.offsets[k + 1]].view(n, n) for k, n in enumerate(self.nbf)]
 
     def herfck_batch(self, dpacked, fpacked=None, hfxfac=1.0, thrs=1e-12, use_graph=True, stream=None,
-                     stats=True):
-        """F = J - hfxfac/2 K of every molecule, packed device tensors."""
+                     stats=True, mixed_cutoff=0.0):
+        """F = J - hfxfac/2 K of every molecule, packed device tensors.  With
+        ``mixed_cutoff`` > 0 the classes that the tuned context splits run
+        their quartets with bound Q_AB Q_CD max|D| below it in FP32."""
         import torch
 
         if fpacked is None:
             fpacked = torch.empty_like(dpacked)
-        opt = _lib.default_options(thrs=float(thrs), hfxfac=float(hfxfac))
+        opt = _lib.default_options(thrs=float(thrs), hfxfac=float(hfxfac), mixed_cutoff=float(mixed_cutoff))
         if stream is None:
             stream = torch.cuda.current_stream(dpacked.device).cuda_stream
         st = _lib.DgfStats()

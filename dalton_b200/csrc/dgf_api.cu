@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "dgf_ctx.h"
+#include "dgf_sph.h"
 #include "dgf_md.cuh"
 
 using namespace dgf;
@@ -114,62 +115,15 @@ void boys_table_host(std::vector<double> &out) {
 
 // Cartesian -> real spherical coefficients with Dalton's conventions (SPHCO1,
 // DALTON/abacus/her1pro.F:4697-4770, MORDER=1 so m = -l..l, MINTEG=2 so the
-// functions are normalised given Cartesians carrying the x^l norm); p and s
-// are identities.  Layout per l: rows m, columns Cartesian components.
+// functions are normalised given Cartesians carrying the x^l norm), from the
+// compile-time generator the kernels' immediate coefficients come from; p
+// and s are identities.  Layout per l: rows m, columns Cartesian components.
 void sph_table_host(std::vector<double> &out) {
   out.assign(kSphTableDoubles, 0.0);
-  auto binom = [](int nn, int k) {
-    if (k < 0 || k > nn) return 0.0;
-    double r = 1.0;
-    for (int i = 1; i <= k; ++i) r = r * (nn - k + i) / i;
-    return r;
-  };
-  auto fact = [](int nn) {
-    double r = 1.0;
-    for (int i = 2; i <= nn; ++i) r *= i;
-    return r;
-  };
   for (int l = 0; l <= kMaxShellL + 1; ++l) {
-    const int nx = ncart(l), nlm = 2 * l + 1;
-    double *T = out.data() + sph_offset(l);
-    if (l <= 1) {
-      for (int i = 0; i < nx; ++i) T[i * nx + i] = 1.0;
-      continue;
-    }
-    std::vector<double> pl(l + 2, 0.0), cs((l + 1) * (l + 1), 0.0);
-    for (int k = 0; k <= l / 2; ++k)
-      pl[l - 2 * k] = ((k % 2) ? -1.0 : 1.0) * std::ldexp(1.0, -l) * binom(l, k) * binom(2 * (l - k), l);
-    cs[0] = 1.0;
-    for (int m = 1; m <= l; ++m) {
-      cs[m * (l + 1)] = 1.0;
-      for (int k = 1; k <= m; ++k) {
-        cs[m * (l + 1) + k] = cs[(m - 1) * (l + 1) + k - 1] * (((k - 1) % 2) ? -1.0 : 1.0);
-        if (m > k) cs[m * (l + 1) + k] += cs[(m - 1) * (l + 1) + k];
-      }
-    }
-    double df = 1.0;
-    for (int v = 2 * l - 1; v > 0; v -= 2) df *= v;
-    for (int m = 0; m <= l; ++m) {
-      double cm = (m == 0) ? 1.0 : std::sqrt(2.0 * fact(l - m) / fact(l + m));
-      cm /= std::sqrt(df);
-      for (int k = (l - m) % 2; k <= l - m; k += 2) {
-        if (m > 0) pl[k] = (k + 1) * pl[k + 1];
-        const double cmk = cm * pl[k];
-        for (int i = 0; i <= (l - k - m) / 2; ++i) {
-          const double cmki = cmk * binom((l - k - m) / 2, i);
-          for (int j = 0; j <= i; ++j) {
-            const double cmkij = cmki * binom(i, j);
-            for (int nn = 0; nn <= m; ++nn) {
-              int ix = l - 2 * j - m + nn;
-              ix = ix * (ix + 1) / 2 + l + 1 - m - 2 * i;  // 1-based Cartesian index
-              const int ilm = (nn % 2 == 1) ? (l - m) : (l + m);  // 0-based row
-              T[ilm * nx + (ix - 1)] += cmkij * cs[m * (l + 1) + nn];
-            }
-          }
-        }
-      }
-    }
-    (void)nlm;
+    const sph::Table t = sph::make(l);
+    const int n = (2 * l + 1) * ncart(l);
+    for (int k = 0; k < n; ++k) out[sph_offset(l) + k] = t.c[k];
   }
 }
 
@@ -244,7 +198,11 @@ static int launch_kernel(dgf_ctx *c, const ClassKernel &k, int X, int Y, JKArgs 
     r.lc = cls_l1(Y);
     r.ld = Y - r.lc * (r.lc + 1) / 2;
     r.precision = (precision == 1) ? 32 : 64;
-    r.kernel = thread_kernel ? 0 : k.kind == kKindWarpTeam ? 2 : k.kind == kKindWarp ? 4 : 1;
+    r.kernel = thread_kernel                 ? 0
+               : k.kind == kKindWarpTeam   ? 2
+               : k.kind == kKindWarp       ? 4
+               : k.kind == kKindWarpMma    ? 6
+                                           : 1;
     (void)k;
     r.quartets = args.nquartet - args.q_begin;
     r.evaluated = 0;
@@ -1394,6 +1352,22 @@ extern "C" const char *dgf_last_error(void) { return dgf::g_last_error.c_str(); 
 extern "C" int dgf_copy_tuning(dgf_ctx *dst, const dgf_ctx *src) {
   if (!dst || !src) DGF_FAIL(DGF_ERR_ARG, "NULL context");
   memcpy(dst->choice, src->choice, sizeof(dst->choice));
+  memcpy(dst->split_ok, src->split_ok, sizeof(dst->split_ok));
+  return DGF_OK;
+}
+
+extern "C" int dgf_set_class_kernel(dgf_ctx *c, int la, int lb, int lc, int ld, int precision, int variant) {
+  if (!c) DGF_FAIL(DGF_ERR_ARG, "NULL context");
+  if (la < lb || lc < ld || lb < 0 || ld < 0 || la > kMaxShellL || lc > kMaxShellL)
+    DGF_FAIL(DGF_ERR_ARG, "class angular momenta must satisfy la >= lb >= 0, lc >= ld >= 0, at most f");
+  if (precision != 64 && precision != 32) DGF_FAIL(DGF_ERR_ARG, "precision must be 64 or 32");
+  int X = la * (la + 1) / 2 + lb, Y = lc * (lc + 1) / 2 + ld;
+  if (X < Y) std::swap(X, Y);
+  const int p = precision == 32 ? 1 : 0;
+  const bool bra1 = c->cls_max_npp[X] == 1;
+  if (!jk_kernel_variant(X, Y, p, variant, false, bra1).launch && !jk_kernel_variant(X, Y, p, variant, true, bra1).launch)
+    DGF_FAIL(DGF_ERR_UNSUPPORTED, "no such kernel variant for this class and precision");
+  c->choice[X][Y][p] = variant;
   return DGF_OK;
 }
 
@@ -1454,7 +1428,7 @@ extern "C" int dgf_autotune(dgf_ctx *c, const double *dmat_device, const dgf_opt
       // single-primitive launches, the cooperative kernels are not timed
       // (they are several times slower wherever both exist).
       const bool has_warp = bra1 && jk_kernel_variant(cp.X, cp.Y, p, -3, true, bra1).launch != nullptr;
-      for (int v = -3; v < kThreadVariants; ++v) {
+      for (int v = -4; v < kThreadVariants; ++v) {
         if (!jk_kernel_variant(cp.X, cp.Y, p, v, false, bra1).launch &&
             !jk_kernel_variant(cp.X, cp.Y, p, v, true, bra1).launch)
           continue;

@@ -1,6 +1,9 @@
 // Batched Fock builds (pattern 2): many molecules of uneven size evaluated
 // by one launch per quartet class over a merged, class-sorted quartet queue,
-// the whole sequence captured once as a CUDA graph and replayed.
+// the launches spread over forked streams (so that their tails overlap) and
+// the whole sequence captured once as a CUDA graph and replayed.  The mixed
+// form splits the classes the tuned context splits into FP64 and FP32
+// launches, with per-shell-pair density bounds of every molecule.
 //
 // Every molecule keeps its own canonical quartet list (no cross-molecule
 // quartets): the merged pair list of a class is the concatenation of the
@@ -59,10 +62,28 @@ struct dgf_batch {
   cudaGraphExec_t exec = nullptr;
   const double *g_in = nullptr;
   double *g_out = nullptr;
-  double g_thrs = -1.0, g_hfx = 0.0;
+  double g_thrs = -1.0, g_hfx = 0.0, g_mixed = 0.0;
   cudaStream_t g_stream = nullptr;
   int64_t launches = 0;
   int choice[kNumPairClass][kNumPairClass] = {};  // FP64 kernel per class pair (from the largest context)
+  int choice32[kNumPairClass][kNumPairClass] = {};  // FP32 kernel per class pair (mixed form)
+  int split_ok[kNumPairClass][kNumPairClass] = {};  // mixed form: split the class into FP64 + FP32 launches
+  int cls_max_npp[kNumPairClass] = {};             // most primitive pairs of any pair of the class
+  // mixed form: working shells of all molecules (first function | count),
+  // per molecule {shell offset, shells, working functions} and the prefix
+  // sums of shells^2, and the shell-pair maxima of |D| in the packed
+  // working-matrix layout (allocated on the first mixed call)
+  int *d_bsh = nullptr, *d_bmol = nullptr;
+  int64_t *d_bpref = nullptr;
+  int64_t nshpair = 0;
+  int nshell_all = 0;
+  float *d_dmw = nullptr;
+  // The class launches are spread over kBatchStreams streams forked from
+  // the caller's (or the capture) stream and joined back before the
+  // epilogue, so that the tail of one launch overlaps the next ones.
+  static constexpr int kBatchStreams = 4;
+  cudaStream_t aux[kBatchStreams] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kBatchStreams] = {};
 };
 
 static void batch_free(dgf_batch *b) {
@@ -70,11 +91,17 @@ static void batch_free(dgf_batch *b) {
   DeviceGuard g(b->device);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  void *ptrs[] = {b->d_pairs, b->d_pp, b->d_boys, b->d_sph, b->d_offsets, b->d_dims, b->d_wmap_i, b->d_wmap_c,
-                  b->d_D,     b->d_Ds, b->d_Fh,   b->d_cnt, b->d_qoff,    b->d_kbase};
+  void *ptrs[] = {b->d_pairs, b->d_pp,  b->d_boys, b->d_sph,  b->d_offsets, b->d_dims,  b->d_wmap_i,
+                  b->d_wmap_c, b->d_D,   b->d_Ds,   b->d_Fh,   b->d_cnt,     b->d_qoff,  b->d_kbase,
+                  b->d_bsh,    b->d_bmol, b->d_bpref, b->d_dmw};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
+  for (int k = 0; k < dgf_batch::kBatchStreams; ++k) {
+    if (b->aux[k]) cudaStreamDestroy(b->aux[k]);
+    if (b->ev_join[k]) cudaEventDestroy(b->ev_join[k]);
+  }
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   delete b;
@@ -118,7 +145,11 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
   for (dgf_int m = 1; m < nmol; ++m)
     if (ctxs[m]->nbf > ctxs[big]->nbf) big = m;
   for (int X = 0; X < kNumPairClass; ++X)
-    for (int Y = 0; Y < kNumPairClass; ++Y) b->choice[X][Y] = ctxs[big]->choice[X][Y][0];
+    for (int Y = 0; Y < kNumPairClass; ++Y) {
+      b->choice[X][Y] = ctxs[big]->choice[X][Y][0];
+      b->choice32[X][Y] = ctxs[big]->choice[X][Y][1];
+      b->split_ok[X][Y] = ctxs[big]->split_ok[X][Y];
+    }
   // Concatenated AO <-> working maps (offsets made global, indices stay local).
   std::vector<int> wr_off{0}, wr_idx, ac_off{0}, ac_idx, wbase, abase;
   std::vector<double> wr_c, ac_c;
@@ -177,7 +208,26 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
     }
   }
   b->cls_off[kNumPairClass] = (int)b->pairs.size();
-  const size_t n_boys = (size_t)(kBoysMaxM + 1) * kBoysTableDoubles;
+  std::vector<int> bsh, bmol;
+  std::vector<int64_t> bpref{0};
+  {
+    std::vector<int> nf;
+    for (dgf_int m = 0; m < nmol; ++m) {
+      const dgf_ctx *c = ctxs[m];
+      bmol.push_back((int)(bsh.size()));
+      bmol.push_back(c->nwshell);
+      bmol.push_back(c->nwf);
+      bsh.insert(bsh.end(), c->ws_ao.begin(), c->ws_ao.end());
+      for (int k = 0; k < c->nwshell; ++k) nf.push_back(nfun(c->ws_l[k], c->spherical));
+      bpref.push_back(bpref.back() + (int64_t)c->nwshell * c->nwshell);
+    }
+    bsh.insert(bsh.end(), nf.begin(), nf.end());  // first functions, then counts
+  }
+  b->nshpair = bpref.back();
+  b->nshell_all = (int)(bsh.size() / 2);
+  for (int X = 0; X < kNumPairClass; ++X)
+    for (int i = b->cls_off[X]; i < b->cls_off[X + 1]; ++i) b->cls_max_npp[X] = std::max(b->cls_max_npp[X], b->pairs[i].npp);
+  const size_t n_boys = kBoysAllDoubles;  // full-degree and low-degree (FP32 half) tables
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void **p, size_t bytes) {
     if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 8));
@@ -194,6 +244,9 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
   alloc((void **)&b->d_Ds, b->total_w * 8);
   alloc((void **)&b->d_Fh, b->total_w * 8);
   alloc((void **)&b->d_cnt, 4 * kCounterSlots * 8);
+  alloc((void **)&b->d_bsh, bsh.size() * 4);
+  alloc((void **)&b->d_bmol, bmol.size() * 4);
+  alloc((void **)&b->d_bpref, bpref.size() * 8);
   if (e != cudaSuccess) {
     cudaGetLastError();
     batch_free(b);
@@ -207,7 +260,15 @@ extern "C" int dgf_batch_create(dgf_ctx *const *ctxs, dgf_int nmol, dgf_batch **
   if (e == cudaSuccess) e = cudaMemcpy(b->d_dims, dims.data(), dims.size() * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_wmap_i, ints.data(), ints.size() * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && !cs.empty()) e = cudaMemcpy(b->d_wmap_c, cs.data(), cs.size() * 8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_bsh, bsh.data(), bsh.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_bmol, bmol.data(), bmol.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_bpref, bpref.data(), bpref.size() * 8, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  for (int k = 0; k < dgf_batch::kBatchStreams; ++k) {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join[k], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
   if (e != cudaSuccess) {
@@ -319,10 +380,55 @@ static int batch_plan(dgf_batch *b, double thrs) {
   return DGF_OK;
 }
 
-static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double hfx, cudaStream_t st) {
+// Mixed form of a batch: max |D| over the working functions of every shell
+// pair of every molecule (both orientations), rounded up to FP32 and stored
+// at (first function of A, first function of B) of the molecule's block of
+// the packed working matrix.  e runs over the molecules' shell pairs;
+// pref holds the prefix sums of shells^2, mol {shell offset, shells,
+// functions} per molecule, sh the shells' first functions then counts.
+__global__ void batch_dmax_kernel(const double *__restrict__ D, const int64_t *__restrict__ woff,
+                                  const int64_t *__restrict__ pref, const int *__restrict__ mol,
+                                  const int *__restrict__ sh, int nshell_all, int nmol, int64_t npair,
+                                  float *__restrict__ dm) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < npair; e += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nmol - 1;  // the molecule: last m with pref[m] <= e
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pref[mid] <= e) lo = mid; else hi = mid - 1;
+    }
+    const int m = lo, s0 = mol[3 * m], ns = mol[3 * m + 1], n = mol[3 * m + 2];
+    const int64_t local = e - pref[m];
+    const int A = s0 + (int)(local / ns), B = s0 + (int)(local % ns);
+    const int pa = sh[A], na = sh[nshell_all + A], pb = sh[B], nb = sh[nshell_all + B];
+    const double *Dm = D + woff[m];
+    double v = 0.0;
+    for (int i = 0; i < na; ++i)
+      for (int j = 0; j < nb; ++j) {
+        const int p = pa + i, q = pb + j;
+        v = fmax(v, fmax(fabs(Dm[(size_t)p * n + q]), fabs(Dm[(size_t)q * n + p])));
+      }
+    dm[woff[m] + (int64_t)pa * n + pb] = __double2float_ru(v);
+  }
+}
+
+// la + lb of pair class X (classes ordered (s,s), (p,s), (p,p), (d,s), ...).
+static int pair_class_l(int X) {
+  const int la = (X == 0) ? 0 : (X <= 2) ? 1 : (X <= 5) ? 2 : 3;
+  return la + (X - la * (la + 1) / 2);
+}
+
+static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double hfx, double mixed_cutoff,
+                         cudaStream_t st) {
   int64_t launches = 0;
   launch_work_prep(b->maps, din, b->d_D, b->d_Ds, 2, b->total_w, b->nsm, st);  // symmetric part, IFCTYP 13
   ++launches;
+  const bool mixed = mixed_cutoff > 0.0;
+  if (mixed) {
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(b->nshpair / 128 + 1, (int64_t)b->nsm * 8));
+    batch_dmax_kernel<<<grid, 128, 0, st>>>(b->d_D, b->d_offsets + b->nmol + 1, b->d_bpref, b->d_bmol, b->d_bsh,
+                                             b->nshell_all, b->nmol, b->nshpair, b->d_dmw);
+    ++launches;
+  }
   if (cudaMemsetAsync(b->d_Fh, 0, b->total_w * 8, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "memset failed");
   JKArgs a;
   memset(&a, 0, sizeof(a));
@@ -336,10 +442,39 @@ static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double h
   a.Fh = b->d_Fh;
   a.jscale[0] = 1.0;
   a.kscale[0] = 0.5 * hfx;
-  a.schwarz_thr = b->plan_thrs;
-  a.ket_pp0 = -1;  // a molecule's kets are not adjacent to the next molecule's  // the plan's last Schwarz bin may reach below the threshold
+  a.schwarz_thr = b->plan_thrs;  // the plan's last Schwarz bin may reach below the threshold
+  a.ket_pp0 = -1;                 // a molecule's kets are not adjacent to the next molecule's
+  a.dmax_w = mixed ? b->d_dmw : nullptr;
+  a.split = mixed_cutoff;
+  // Longest-first assignment of the plan entries to the forked streams by
+  // model cost (quartets x a per-class weight).
+  const int ns = dgf_batch::kBatchStreams;
+  std::vector<int> order(b->plan.size()), stream_of(b->plan.size(), 0);
+  std::vector<double> cost(b->plan.size());
+  for (size_t i = 0; i < b->plan.size(); ++i) {
+    const BatchPlan &bp = b->plan[i];
+    const int L = pair_class_l(bp.X) + pair_class_l(bp.Y);
+    cost[i] = (double)bp.nquartet * (double)n3(L) * (double)(1 << std::min(bp.bucket, 6));
+    order[i] = (int)i;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int u, int v) { return cost[u] > cost[v]; });
+  {
+    double load[dgf_batch::kBatchStreams] = {};
+    for (int i : order) {
+      int k = 0;
+      for (int t = 1; t < ns; ++t)
+        if (load[t] < load[k]) k = t;
+      stream_of[i] = k;
+      load[k] += cost[i];
+    }
+  }
+  if (cudaEventRecord(b->ev_fork, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "event record failed");
+  for (int k = 0; k < ns; ++k)
+    if (cudaStreamWaitEvent(b->aux[k], b->ev_fork, 0) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "stream fork failed");
   int slot = 0;
-  for (const BatchPlan &bp : b->plan) {
+  for (int i : order) {
+    const BatchPlan &bp = b->plan[i];
+    cudaStream_t ls = b->aux[stream_of[i]];
     a.bra = b->d_pairs + b->cls_off[bp.X];
     a.ket = b->d_pairs + b->cls_off[bp.Y];
     a.ket_off = 0;
@@ -349,20 +484,34 @@ static int batch_enqueue(dgf_batch *b, const double *din, double *fout, double h
     a.kbase = b->d_kbase + bp.koff;
     a.q_begin = 0;
     a.nquartet = bp.nquartet;
-    a.counters = b->d_cnt + 4 * (slot++ % kCounterSlots);
-    const int la = (bp.X == 0) ? 0 : (bp.X <= 2) ? 1 : (bp.X <= 5) ? 2 : 3;
-    const int lb = bp.X - la * (la + 1) / 2;
-    const int lc = (bp.Y == 0) ? 0 : (bp.Y <= 2) ? 1 : (bp.Y <= 5) ? 2 : 3;
-    const int ld = bp.Y - lc * (lc + 1) / 2;
-    a.boys = b->d_boys + (size_t)(la + lb + lc + ld) * kBoysTableDoubles;
-    const ClassKernel *kp = &jk_kernel_variant(bp.X, bp.Y, 0, b->choice[bp.X][bp.Y], bp.bucket == 0);
-    if (!kp->launch) kp = &jk_kernel(bp.X, bp.Y, 0, bp.bucket == 0);
-    const ClassKernel &k = *kp;
-    const int64_t per_block = k.qpb;
-    const int grid = (int)std::max<int64_t>(
-        1, std::min<int64_t>((bp.nquartet + per_block - 1) / per_block, (int64_t)b->nsm * 16));
-    k.launch(a, grid, k.block, k.smem, st);
-    ++launches;
+    const int Lq = pair_class_l(bp.X) + pair_class_l(bp.Y);
+    const bool bra1 = b->cls_max_npp[bp.X] == 1;
+    const ClassKernel *kp = &jk_kernel_variant(bp.X, bp.Y, 0, b->choice[bp.X][bp.Y], bp.bucket == 0, bra1);
+    if (!kp->launch) kp = &jk_kernel(bp.X, bp.Y, 0, bp.bucket == 0, bra1);
+    // Mixed form: the classes the tuned context splits run an FP64 launch
+    // for quartets whose bound is at or above the cutoff and an FP32 launch
+    // for the rest.
+    const ClassKernel *k32 = nullptr;
+    if (mixed && b->split_ok[bp.X][bp.Y]) {
+      k32 = &jk_kernel_variant(bp.X, bp.Y, 1, b->choice32[bp.X][bp.Y], bp.bucket == 0, bra1);
+      if (!k32->launch) k32 = &jk_kernel(bp.X, bp.Y, 1, bp.bucket == 0, bra1);
+      if (!k32->launch) k32 = nullptr;
+    }
+    for (int part = 0; part < (k32 ? 2 : 1); ++part) {
+      const ClassKernel &k = part ? *k32 : *kp;
+      a.mode = k32 ? 1 + part : 0;
+      a.boys = b->d_boys + (part ? boys_low_offset(Lq) : (size_t)Lq * kBoysTableDoubles);
+      a.counters = b->d_cnt + 4 * (slot++ % kCounterSlots);
+      const int64_t per_block = k.qpb;
+      const int grid = (int)std::max<int64_t>(
+          1, std::min<int64_t>((bp.nquartet + per_block - 1) / per_block, (int64_t)b->nsm * 16));
+      k.launch(a, grid, k.block, k.smem, ls);
+      ++launches;
+    }
+  }
+  for (int k = 0; k < ns; ++k) {
+    if (cudaEventRecord(b->ev_join[k], b->aux[k]) != cudaSuccess || cudaStreamWaitEvent(st, b->ev_join[k], 0) != cudaSuccess)
+      BFAIL(DGF_ERR_CUDA, "stream join failed");
   }
   launch_work_combine(b->maps, b->d_Fh, b->d_Fh, fout, 1.0, b->total, b->nsm, st);  // F = C^T (Fh + Fh^T) C
   ++launches;
@@ -378,8 +527,16 @@ extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, do
   dgf_options o;
   dgf_default_options(&o);
   if (opt) o = *opt;
-  if (o.ifthrs < 16 || o.mixed_cutoff > 0.0 || o.shard_count > 1 || o.hfxmu != 0.0)
+  if (o.ifthrs < 16 || o.shard_count > 1 || o.hfxmu != 0.0)
     BFAIL(DGF_ERR_UNSUPPORTED, "batched builds take the Schwarz-screened form without range separation only");
+  if (!(o.mixed_cutoff >= 0.0)) BFAIL(DGF_ERR_ARG, "mixed_cutoff must be >= 0");
+  if (o.mixed_cutoff > 0.0 && !b->d_dmw) {
+    if (cudaMalloc(&b->d_dmw, std::max<int64_t>(b->total_w, 1) * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      b->d_dmw = nullptr;
+      BFAIL(DGF_ERR_NOMEM, "device allocation of the batch density bounds failed");
+    }
+  }
   cudaStream_t st = (cudaStream_t)stream;  // NULL: the legacy default stream, as in dgf_fock_device
   int r = batch_plan(b, o.thrs);
   if (r) return r;
@@ -387,7 +544,8 @@ extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, do
   if (cudaEventRecord(b->ev0, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "event record failed");
   if (use_graph) {
     const bool stale = !b->exec || b->g_in != dmat_packed_device || b->g_out != fmat_packed_device ||
-                       b->g_thrs != o.thrs || b->g_hfx != o.hfxfac || b->g_stream != st;
+                       b->g_thrs != o.thrs || b->g_hfx != o.hfxfac || b->g_mixed != o.mixed_cutoff ||
+                       b->g_stream != st;
     if (stale) {
       if (b->exec) {
         cudaGraphExecDestroy(b->exec);
@@ -399,7 +557,7 @@ extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, do
       cudaStream_t cs = b->stream;
       if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         BFAIL(DGF_ERR_CUDA, "stream capture failed to begin");
-      r = batch_enqueue(b, dmat_packed_device, fmat_packed_device, o.hfxfac, cs);
+      r = batch_enqueue(b, dmat_packed_device, fmat_packed_device, o.hfxfac, o.mixed_cutoff, cs);
       cudaGraph_t gr = nullptr;
       cudaError_t e = cudaStreamEndCapture(cs, &gr);
       if (r) {
@@ -417,11 +575,12 @@ extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, do
       b->g_out = fmat_packed_device;
       b->g_thrs = o.thrs;
       b->g_hfx = o.hfxfac;
+      b->g_mixed = o.mixed_cutoff;
       b->g_stream = st;
     }
     if (cudaGraphLaunch(b->exec, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "graph launch failed");
   } else {
-    r = batch_enqueue(b, dmat_packed_device, fmat_packed_device, o.hfxfac, st);
+    r = batch_enqueue(b, dmat_packed_device, fmat_packed_device, o.hfxfac, o.mixed_cutoff, st);
     if (r) return r;
   }
   if (cudaEventRecord(b->ev1, st) != cudaSuccess) BFAIL(DGF_ERR_CUDA, "event record failed");
@@ -437,8 +596,8 @@ extern "C" int dgf_fock_batch(dgf_batch *b, const double *dmat_packed_device, do
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     stats->quartets_total = tq;
-    stats->quartets_fp64 = (int64_t)s[0];
-    stats->quartets_fp32 = 0;
+    stats->quartets_fp64 = (int64_t)(s[0] - s[3]);
+    stats->quartets_fp32 = (int64_t)s[3];
     stats->quartets_skipped = 0;
     stats->prim_quartets = (int64_t)s[1];
     stats->kernel_launches = b->launches;

@@ -115,6 +115,10 @@ struct JKArgs {
   double kscale[kMaxSlots];
   // screening / precision split
   const float *dmax;        // [nshell*nshell] max |D| per shell pair, or null
+  // batches: max |D| per shell pair stored in the packed working-matrix
+  // layout, at (first function of A, first function of B) of the pair's
+  // molecule (offset dbase, stride nbfm); null: dmax above
+  const float *dmax_w;
   int nshell;
   double dens_thr;          // skip if bound < dens_thr (0: no density screening)
   double split;             // precision split bound
@@ -163,7 +167,7 @@ constexpr int kSphTableDoubles = 1 * 1 + 3 * 3 + 5 * 6 + 7 * 10 + 9 * 15;
 
 typedef void (*JKLauncher)(const JKArgs &, int grid, int block, size_t smem, cudaStream_t);
 
-enum { kKindThread = 0, kKindTeam = 1, kKindWarpTeam = 2, kKindWarp = 4 };
+enum { kKindThread = 0, kKindTeam = 1, kKindWarpTeam = 2, kKindWarp = 4, kKindWarpMma = 6 };
 
 struct ClassKernel {
   JKLauncher launch;
@@ -171,7 +175,7 @@ struct ClassKernel {
   size_t smem;   // dynamic shared memory (team and warp kernels); 0 for thread kernels
   int chunks;    // thread kernels: A-component chunks (grid.y)
   int qpb;       // quartets a block works on at a time (grid sizing)
-  int kind;      // kKindThread, kKindTeam, kKindWarpTeam or kKindWarp
+  int kind;      // kKindThread, kKindTeam, kKindWarpTeam, kKindWarp or kKindWarpMma
 };
 
 constexpr int kThreadVariants = 2;

@@ -14,13 +14,17 @@ namespace {
 const ClassKernel kNone{nullptr, 0, 0, 0, 0, 0};
 }
 
-// variant: -3 = warp-per-quartet kernel, -2 = warp-team kernel, -1 = team
-// kernel, 0.. = thread-kernel variant; precision 0 = FP64, 1 = FP32.
+// variant: -4 = warp-per-quartet kernel with FP64 tensor-core (DMMA)
+// transforms (any pairs), -3 = warp-per-quartet kernel (for launches whose pairs have one
+// primitive pair each, or any launch of a class whose warp kernel loops over
+// primitives), -2 = warp-team kernel, -1 = team kernel, 0.. = thread-kernel
+// variant; precision 0 = FP64, 1 = FP32.
 // Returns a kernel with launch == nullptr when absent.
 const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1, bool bra1) {
   const JKEntry &e = g_jk_table[X][Y];
   const int p = precision ? 1 : 0;
-  if (variant == -3) return (ket1 && bra1) ? e.warp[p] : kNone;
+  if (variant == -4) return precision == 0 ? e.warp_mma : kNone;
+  if (variant == -3) return ((ket1 && bra1) || e.warp_mp) ? e.warp[p] : kNone;
   if (variant == -2) return precision == 0 ? e.wteam : kNone;
   if (variant < 0) return precision == 0 ? e.team : kNone;
   if (variant >= kThreadVariants) return kNone;

@@ -17,7 +17,9 @@ struct JKEntry {
   ClassKernel wteam;                     // one quartet per warp (light quartets), when it fits
   ClassKernel thr[2][kThreadVariants];   // [precision 0 = FP64, 1 = FP32][variant]
   ClassKernel thr1[2][kThreadVariants];  // same, for kets of one primitive pair each
-  ClassKernel warp[2];                   // warp-per-quartet kernel [FP64, FP32] (single primitive pairs)
+  ClassKernel warp[2];                   // warp-per-quartet kernel [FP64, FP32]
+  bool warp_mp;                          // the warp kernel loops over primitive pairs (else one per side only)
+  ClassKernel warp_mma;                  // warp-per-quartet kernel with DMMA transforms (FP64, any pairs)
   cudaError_t (*prepare[3])();           // one per generated part
 };
 

@@ -27,21 +27,22 @@ constexpr bool warp_eligible() {
   }
 }
 
-template <int LA, int LB, int LC, int LD, typename T>
+template <int LA, int LB, int LC, int LD, typename T, bool MMA>
 void launch_warp(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
-  jk_warp_kernel<LA, LB, LC, LD, T><<<grid, block, smem, s>>>(a);
+  jk_warp_kernel<LA, LB, LC, LD, T, MMA><<<grid, block, smem, s>>>(a);
 }
 
-template <int LA, int LB, int LC, int LD, typename T>
+template <int LA, int LB, int LC, int LD, typename T, bool MMA = false>
 ClassKernel warp_entry() {
   using W = wq::Shape<LA, LB, LC, LD, T>;
-  return ClassKernel{&launch_warp<LA, LB, LC, LD, T>, 32 * W::WPB, W::smem(W::WPB), 1, W::WPB, kKindWarp};
+  return ClassKernel{&launch_warp<LA, LB, LC, LD, T, MMA>, 32 * W::WPB, W::smem(W::WPB), 1, W::WPB,
+                     MMA ? kKindWarpMma : kKindWarp};
 }
 
-template <int LA, int LB, int LC, int LD, typename T>
+template <int LA, int LB, int LC, int LD, typename T, bool MMA = false>
 cudaError_t prepare_warp() {
   using W = wq::Shape<LA, LB, LC, LD, T>;
-  return cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD, T, MMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)W::smem(W::WPB));
 }
 
@@ -58,6 +59,8 @@ cudaError_t prepare_team() {
   if constexpr (warp_eligible<LA, LB, LC, LD>()) {
     if (e == cudaSuccess) e = prepare_warp<LA, LB, LC, LD, double>();
     if (e == cudaSuccess) e = prepare_warp<LA, LB, LC, LD, float>();
+    if constexpr (wq::Shape<LA, LB, LC, LD, double>::MMA_OK)
+      if (e == cudaSuccess) e = prepare_warp<LA, LB, LC, LD, double, true>();
   }
   return e;
 }
@@ -77,6 +80,8 @@ void fill_team() {
   if constexpr (warp_eligible<LA, LB, LC, LD>()) {
     e.warp[0] = warp_entry<LA, LB, LC, LD, double>();
     e.warp[1] = warp_entry<LA, LB, LC, LD, float>();
+    e.warp_mp = wq::Shape<LA, LB, LC, LD, double>::MP && wq::Shape<LA, LB, LC, LD, float>::MP;
+    if constexpr (wq::Shape<LA, LB, LC, LD, double>::MMA_OK) e.warp_mma = warp_entry<LA, LB, LC, LD, double, true>();
   }
 }
 

@@ -224,7 +224,7 @@ constexpr int kThreadBlock = 256;
 constexpr int kThreadWarps = kThreadBlock / 32;
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
-__device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, const double *sph, Tc *ebra,
+__device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, Tc *ebra,
                                                unsigned long long &cnt_q, unsigned long long &cnt_p,
                                                unsigned long long &cnt_s) {
   constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD;
@@ -449,67 +449,28 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
 #pragma unroll
     for (int k = 0; k < NACC; ++k) g[k] = (double)acc[k];
     if (SPH_NEEDED && sphr && work) {
+      // index by index with compile-time coefficients (SPHCO1 convention)
       double tmp[NOUT];
-      if (LA >= 2) {
-        const double *T = sph + sph_offset(LA);
-#pragma unroll
-        for (int o = 0; o < FAc; ++o)
-#pragma unroll
-          for (int r = 0; r < NB * NCD; ++r) {
-            double s = 0.0;
-#pragma unroll
-            for (int x = 0; x < NAc; ++x) s += T[o * NA + A0 + x] * g[x * NB * NCD + r];
-            tmp[o * NB * NCD + r] = s;
-          }
+      if constexpr (LA >= 2) {
+        sph_index<LA, 1, NAc, A0, NB * NCD>(g, tmp);
 #pragma unroll
         for (int k = 0; k < FAc * NB * NCD; ++k) g[k] = tmp[k];
       }
       constexpr int A1r = (LA >= 2) ? FAc : NAc;
-      if (LB >= 2) {
-        const double *T = sph + sph_offset(LB);
-#pragma unroll
-        for (int i = 0; i < A1r; ++i)
-#pragma unroll
-          for (int o = 0; o < FBc; ++o)
-#pragma unroll
-            for (int r = 0; r < NCD; ++r) {
-              double s = 0.0;
-#pragma unroll
-              for (int x = 0; x < NB; ++x) s += T[o * NB + x] * g[(i * NB + x) * NCD + r];
-              tmp[(i * FBc + o) * NCD + r] = s;
-            }
+      if constexpr (LB >= 2) {
+        sph_index<LB, A1r, NB, 0, NCD>(g, tmp);
 #pragma unroll
         for (int k = 0; k < A1r * FBc * NCD; ++k) g[k] = tmp[k];
       }
       constexpr int AB1 = A1r * ((LB >= 2) ? FBc : NB);
-      if (LC >= 2) {
-        const double *T = sph + sph_offset(LC);
-#pragma unroll
-        for (int i = 0; i < AB1; ++i)
-#pragma unroll
-          for (int o = 0; o < FCc; ++o)
-#pragma unroll
-            for (int r = 0; r < ND; ++r) {
-              double s = 0.0;
-#pragma unroll
-              for (int x = 0; x < NC; ++x) s += T[o * NC + x] * g[(i * NC + x) * ND + r];
-              tmp[(i * FCc + o) * ND + r] = s;
-            }
+      if constexpr (LC >= 2) {
+        sph_index<LC, AB1, NC, 0, ND>(g, tmp);
 #pragma unroll
         for (int k = 0; k < AB1 * FCc * ND; ++k) g[k] = tmp[k];
       }
       constexpr int ABC1 = AB1 * ((LC >= 2) ? FCc : NC);
-      if (LD >= 2) {
-        const double *T = sph + sph_offset(LD);
-#pragma unroll
-        for (int i = 0; i < ABC1; ++i)
-#pragma unroll
-          for (int o = 0; o < FDc; ++o) {
-            double s = 0.0;
-#pragma unroll
-            for (int x = 0; x < ND; ++x) s += T[o * ND + x] * g[i * ND + x];
-            tmp[i * FDc + o] = s;
-          }
+      if constexpr (LD >= 2) {
+        sph_index<LD, ABC1, ND, 0, 1>(g, tmp);
 #pragma unroll
         for (int k = 0; k < ABC1 * FDc; ++k) g[k] = tmp[k];
       }
@@ -524,14 +485,14 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
 }
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
-__device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, const double *tab, const double *sph,
+__device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, const double *tab,
                                                    Tc *ebra, unsigned long long &q, unsigned long long &p,
                                                    unsigned long long &s) {
   if constexpr (CH < CA) {
     if (chunk == CH)
-      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, sph, ebra, q, p, s);
+      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, ebra, q, p, s);
     else
-      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, sph, ebra, q, p, s);
+      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, ebra, q, p, s);
   }
 }
 
@@ -554,13 +515,11 @@ __global__ void __launch_bounds__(kThreadBlock, thread_min_blocks(LA + LB + LC +
     jk_thread_kernel(const JKArgs a) {
   constexpr int EA = (LA + 1) * (LB + 1) * (LA + LB + 1);
   __shared__ double tab[kBoysTableDoubles];
-  __shared__ double sph[kSphTableDoubles];
   __shared__ Tc ebra_all[kThreadWarps][3 * EA];
   for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
-  for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
   __syncthreads();
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
-  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, sph, ebra_all[threadIdx.x >> 5], cnt_q, cnt_p,
+  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, ebra_all[threadIdx.x >> 5], cnt_q, cnt_p,
                                                 cnt_s);
   if (a.counters) {
     const int lane = threadIdx.x & 31;

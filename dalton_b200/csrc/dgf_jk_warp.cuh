@@ -23,6 +23,11 @@
 //                    per lane                              (C1SPHR/C2SPHR)
 //   digestion        the six J/K blocks (FCKCON, herfckcon.F:66-80), one
 //                    output element per lane, FP64 atomics
+// Contracted pairs: the bra primitives form the outer loop and the ket
+// primitives the inner one; X sums over the ket primitives and, in the
+// classes where a lane holds a whole ket component column (Shape::MP), each
+// lane sums its column of the (ab|cd) block over the bra primitives in
+// registers (HERMIT's primitive -> contracted step, her2el1.F/her2el2.F).
 // Tc is the arithmetic type of R, the transforms and the tables (double:
 // FP64 drop-in; float: FP32 half of the mixed form); Boys function,
 // prefactor, accumulation across primitive pairs and digestion are FP64.
@@ -91,17 +96,16 @@ constexpr bool chunk_uses(int la, int lb, int i0, int n, int t, int u, int v) {
   return false;
 }
 
-// Calls f(std::integral_constant<int, i>) for i = 0 .. N-1, so that the loop
-// index is a constant expression inside f (index arithmetic and term
-// selection at compile time).
-template <typename F, int... I>
-__device__ __forceinline__ void static_for_impl(F &&f, std::integer_sequence<int, I...>) {
-  (f(std::integral_constant<int, I>{}), ...);
+// One FP64 tensor-core step D(8x8) += A(8x4) B(4x8) (DMMA, mma.sync
+// m8n8k4).  Fragments: lane l holds A[l/4][l%4], B[l%4][l/4] and
+// D[l/4][2(l%4)], D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
 }
-template <int N, typename F>
-__device__ __forceinline__ void static_for(F &&f) {
-  static_for_impl(f, std::make_integer_sequence<int, N>{});
-}
+
+using ::dgf::static_for;
 
 // Per-warp shared memory of class (LA LB | LC LD) in units of 8 bytes.
 template <int LA, int LB, int LC, int LD, typename Tc>
@@ -127,10 +131,27 @@ struct Shape {
   static constexpr int PER_WARP = RA + RB + RT + RD + 8;
   // block-wide: Boys and spherical tables, packed (t,u,v) positions, and the
   // index tables of the bra and ket product tables (ints)
-  static constexpr int COMMON = kBoysTableDoubles + kSphTableDoubles + (N3L + TAB + TCD + 1) / 2;
+  static constexpr int COMMON = kBoysTableDoubles + kSphTableDoubles + (N3L + TAB + TCD + NAB + NCD + 1) / 2;
   static constexpr size_t smem(int warps) { return ((size_t)COMMON + (size_t)warps * PER_WARP) * 8; }
   // warps per block: four when they fit in 100 KB, else two, else one
   static constexpr int WPB = smem(4) <= 100 * 1024 ? 4 : smem(2) <= 100 * 1024 ? 2 : 1;
+  // Primitive loops on both sides: classes whose ket components fit one per
+  // lane and whose bra components fit one register chunk, so that a lane
+  // keeps its column of the (ab|cd) block in registers across the bra
+  // primitives.  Other classes take one primitive pair per side.
+  static constexpr bool MP = NCD <= 32 && NAB <= wq::kChunk;
+  // spherical function counts; SPHR: the MP form applies the spherical
+  // transforms in registers (ket side in the ket transform, bra side when
+  // the block leaves the accumulators)
+  static constexpr int FA = LA >= 2 ? 2 * LA + 1 : NA, FB = LB >= 2 ? 2 * LB + 1 : NB;
+  static constexpr int FC = LC >= 2 ? 2 * LC + 1 : NC, FD = LD >= 2 ? 2 * LD + 1 : ND;
+  static constexpr int FAB = FA * FB, FCD = FC * FD;
+  static constexpr bool SPHR = MP && (LA >= 2 || LB >= 2 || LC >= 2 || LD >= 2);
+  // Tensor-core form (FP64 only): both transforms as DMMA products of dense
+  // tiles, the (ab|cd) block in D fragments across the bra primitives.
+  static constexpr int MT2 = (N3AB + 7) / 8, KT2 = (N3CD + 3) / 4;  // ket product: rows e, depth f
+  static constexpr int MT3 = (NAB + 7) / 8, NT = (NCD + 7) / 8, KT3 = (N3AB + 3) / 4;
+  static constexpr bool MMA_OK = sizeof(Tc) == 8 && MT3 * NT * 2 <= 64;
 };
 
 // One index of the Cartesian -> spherical transform of a block in shared
@@ -168,21 +189,21 @@ __device__ __forceinline__ void sph_pass(const double *in, double *out, const do
 
 }  // namespace wq
 
-// Post-processing and digestion of the Cartesian block Gc[ab][cd] (row
-// stride PG) of one quartet: spherical transform (SPH, index by index
-// between Gc and the scratch block Gs), then the six J/K blocks; Db holds
-// the density blocks.
-template <int LA, int LB, int LC, int LD, typename Tc, bool SPH>
+// Post-processing and digestion of the block Gc[ab][cd] (row stride PG) of
+// one quartet: spherical transform (SPH, index by index between Gc and the
+// scratch block Gs; PRE: the block is spherical already), then the six J/K
+// blocks; Db holds the density blocks.
+template <int LA, int LB, int LC, int LD, typename Tc, bool SPH, bool PRE = false>
 __device__ __forceinline__ void wq_finish(const JKArgs &a, double *Gc, double *Gs, double *Db,
                                           const double *sph, const PairRec &br, const PairRec &kt, int ib, int ic,
                                           double w, int lane) {
   using S = wq::Shape<LA, LB, LC, LD, Tc>;
-  constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NCD = S::NCD, PG = S::PG;
+  constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, PG = S::PG;
   constexpr int FA = (SPH && LA >= 2) ? 2 * LA + 1 : NA, FB = (SPH && LB >= 2) ? 2 * LB + 1 : NB;
   constexpr int FC = (SPH && LC >= 2) ? 2 * LC + 1 : NC, FD = (SPH && LD >= 2) ? 2 * LD + 1 : ND;
   constexpr int FAB = FA * FB, FCD = FC * FD;
   const double *G = Gc;
-  if (SPH) {
+  if (SPH && !PRE) {
     // index by index, ping-pong between Gc and Gs
     constexpr int FA1 = LA >= 2 ? 2 * LA + 1 : NA, FB1 = LB >= 2 ? 2 * LB + 1 : NB;
     constexpr int FC1 = LC >= 2 ? 2 * LC + 1 : NC;
@@ -342,9 +363,27 @@ __device__ __forceinline__ void wq_product_table(const Tc *E, const int *idx, Tc
   }
 }
 
-template <int LA, int LB, int LC, int LD, typename Tc>
+// Packed positions of the three factors of Cartesian component pair ij
+// (i of la, j of lb) in the 1D Hermite tables E (x, y, z blocks of EN
+// entries; the Hermite index t is added by the caller), 10 bits each.
+template <int LA, int LB>
+__device__ __forceinline__ void wq_comp_index(int *idx, int tid, int nt) {
+  constexpr int NB = ncart(LB), NIJ = ncart(LA) * NB, LT = LA + LB + 1, EN = (LA + 1) * (LB + 1) * LT;
+  for (int ij = tid; ij < NIJ; ij += nt) {
+    int ix, iy, iz, jx, jy, jz;
+    cart_decode(LA, ij / NB, ix, iy, iz);
+    cart_decode(LB, ij % NB, jx, jy, jz);
+    idx[ij] = ((ix * (LB + 1) + jx) * LT) | ((EN + (iy * (LB + 1) + jy) * LT) << 10) |
+              ((2 * EN + (iz * (LB + 1) + jz) * LT) << 20);
+  }
+}
+
+// MMA = false: FMA transforms with compact product tables (FP64 and FP32);
+// MMA = true: DMMA transforms (FP64, Shape::MMA_OK classes).
+template <int LA, int LB, int LC, int LD, typename Tc, bool MMA>
 __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
   using S = wq::Shape<LA, LB, LC, LD, Tc>;
+  static_assert(!MMA || S::MMA_OK, "DMMA form of a class it does not fit");
   constexpr int L = S::L, BOX = S::BOX, NAB = S::NAB, NCD = S::NCD, N3AB = S::N3AB,
                 N3CD = S::N3CD, N3L = S::N3L, EA = S::EA, EC = S::EC, PX = S::PX, PG = S::PG;
   extern __shared__ double sm[];
@@ -352,6 +391,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
   double *sph = tab + kBoysTableDoubles;
   int *tuvt = (int *)(sph + kSphTableDoubles);
   int *idx_ab = tuvt + N3L, *idx_cd = idx_ab + S::TAB;
+  int *cmp_ab = idx_cd + S::TCD, *cmp_cd = cmp_ab + NAB;  // packed E positions per Cartesian component pair
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   double *wbase = sm + S::COMMON + (size_t)warp * S::PER_WARP;
   double *regA = wbase, *regB = regA + S::RA;
@@ -368,8 +408,13 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
     tuv_decode(e, t, u, v);
     tuvt[e] = (t * BOX + u) * BOX + v;  // position of (t,u,v) in the R box
   }
-  wq_term_index<LA, LB>(idx_ab, threadIdx.x, blockDim.x);
-  wq_term_index<LC, LD>(idx_cd, threadIdx.x, blockDim.x);
+  if constexpr (MMA) {
+    wq_comp_index<LA, LB>(cmp_ab, threadIdx.x, blockDim.x);
+    wq_comp_index<LC, LD>(cmp_cd, threadIdx.x, blockDim.x);
+  } else {
+    wq_term_index<LA, LB>(idx_ab, threadIdx.x, blockDim.x);
+    wq_term_index<LC, LD>(idx_cd, threadIdx.x, blockDim.x);
+  }
   __syncthreads();
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
   // One contiguous range of the queue per warp.
@@ -405,22 +450,34 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
     if (br.same) w *= 0.5;
     if (kt.same) w *= 0.5;
     if (a.same_class && ib == ic + a.ket_off) w *= 0.5;
-    // Single primitive pair on each side (the host launches this kernel only for such classes).
-    {
-      const PrimPair P1 = load_prim<true>(a.pp + br.pp0);
+    // Primitive pairs: bra i outside, ket j inside.  X accumulates over the
+    // ket primitives; the (ab|cd) block over the bra primitives, in each
+    // lane's registers where one lane holds a whole ket component column
+    // (MP classes; the host launches other classes for one primitive pair
+    // per side only).
+    constexpr bool LOOPS = MMA || S::MP;
+    const int nbp = LOOPS ? br.npp : 1, nkp = LOOPS ? kt.npp : 1;
+    Tc gacc[(S::MP && !MMA) ? NAB : 1];
+#pragma unroll
+    for (int k = 0; k < ((S::MP && !MMA) ? NAB : 1); ++k) gacc[k] = Tc(0);
+    double dacc[MMA ? S::MT3 * S::NT * 2 : 1];  // D fragments of the (ab|cd) block
+#pragma unroll
+    for (int k = 0; k < (MMA ? S::MT3 * S::NT * 2 : 1); ++k) dacc[k] = 0.0;
+    for (int i = 0; i < nbp; ++i) {
+      const PrimPair P1 = load_prim<true>(a.pp + br.pp0 + i);
       __syncwarp();
-      if (tb_bra != ib) {
+      if (nbp > 1 || tb_bra != ib) {
         if (lane < 3) {
           const double pa = lane == 0 ? P1.PAx : lane == 1 ? P1.PAy : P1.PAz;
           const double pb = lane == 0 ? P1.PBx : lane == 1 ? P1.PBy : P1.PBz;
           herm_e<LA, LB, 1, Tc>(Tc(0.5 / P1.p), Tc(pa), Tc(pb), Eb + lane * EA);
         }
         __syncwarp();
-        wq_product_table<S::TAB, Tc>(Eb, idx_ab, Tb, lane);
-        tb_bra = ib;
+        if constexpr (!MMA) wq_product_table<S::TAB, Tc>(Eb, idx_ab, Tb, lane);
+        tb_bra = nbp == 1 ? ib : -1;
       }
-      {
-        const PrimPair P2 = load_prim<true>(a.pp + (a.ket_pp0 >= 0 ? a.ket_pp0 + ic : kt.pp0));
+      for (int j = 0; j < nkp; ++j) {
+        const PrimPair P2 = load_prim<true>(a.pp + (a.ket_pp0 >= 0 ? a.ket_pp0 + ic : kt.pp0 + j));
         __syncwarp();
         if (lane < 3) {
           const double pa = lane == 0 ? P2.PAx : lane == 1 ? P2.PAy : P2.PAz;
@@ -444,7 +501,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
           }
         }
         __syncwarp();
-        wq_product_table<S::TCD, Tc>(Ek, idx_cd, Tk, lane);
+        if constexpr (!MMA) wq_product_table<S::TCD, Tc>(Ek, idx_cd, Tk, lane);
         // R_tuv, level n = L-1 .. 0 from level n+1, ping-pong between R0 and R1
         Tc *prev = R0, *cur = R1;
         if (lane == 0) prev[0] = Tc(Fs[L]);
@@ -477,66 +534,201 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
           cur = sw;
         }
         const Tc *R = prev;
-        // ket transform: lane = bra Hermite index, every ket component (in
-        // chunks of kChunk components, R re-read per chunk)
-        for (int e = lane; e < N3AB; e += 32) {
-          const int base = tuvt[e];
-          wq::static_for<(NCD + wq::kChunk - 1) / wq::kChunk>([&](auto CH_) {
-            constexpr int c0 = decltype(CH_)::value * wq::kChunk;
-            constexpr int nc = NCD - c0 < wq::kChunk ? NCD - c0 : wq::kChunk;
-            Tc xa[nc];
+        if constexpr (MMA) {
+          // ket product X[cd][e] (+)= sum_f R[e+f] E^cd[f]: rows e, columns
+          // cd, depth f; A from the R box, B the dense ket coefficient
+          // products (zero where a component does not reach f).
+          const int g = lane >> 2, t4 = lane & 3;
+          wq::static_for<S::NT>([&](auto NT_) {
+            constexpr int nt = decltype(NT_)::value;
+            const int cd = nt * 8 + g;
+            const int pc = cd < NCD ? cmp_cd[cd] : 0;
+            double bf[S::KT2];
 #pragma unroll
-            for (int k = 0; k < nc; ++k) xa[k] = Tc(0);
-            wq::static_for<N3CD>([&](auto F_) {
-              constexpr int f = decltype(F_)::value;
-              constexpr int ft = wq::tuv_t(f), fu = wq::tuv_u(f), fv = wq::tuv_v(f);
-              if constexpr (wq::chunk_uses(LC, LD, c0, nc, ft, fu, fv)) {
-                const Tc r = R[base + (ft * BOX + fu) * BOX + fv];
-                wq::static_for<nc>([&](auto K_) {
-                  constexpr int cd = c0 + decltype(K_)::value;
-                  if constexpr (wq::uses(LC, LD, cd, ft, fu, fv))
-                    xa[cd - c0] += Tk[wq::term_at(LC, LD, cd, ft, fu, fv)] * r;
+            for (int kk = 0; kk < S::KT2; ++kk) {
+              const int f = kk * 4 + t4;
+              double v = 0.0;
+              if (cd < NCD && f < N3CD) {
+                const int pos = tuvt[f];
+                const int ft = pos / (BOX * BOX), fu = (pos / BOX) % BOX, fv = pos % BOX;
+                v = (double)Ek[(pc & 1023) + ft] * (double)Ek[((pc >> 10) & 1023) + fu] * (double)Ek[(pc >> 20) + fv];
+              }
+              bf[kk] = v;
+            }
+#pragma unroll
+            for (int mt = 0; mt < S::MT2; ++mt) {
+              const int e = mt * 8 + g;
+              const int pe = e < N3AB ? tuvt[e] : 0;
+              double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+              for (int kk = 0; kk < S::KT2; ++kk) {
+                const int f = kk * 4 + t4;
+                const double av = (e < N3AB && f < N3CD) ? (double)R[pe + tuvt[f]] : 0.0;
+                wq::dmma(d0, d1, av, bf[kk]);
+              }
+              const int c0 = nt * 8 + 2 * t4;
+              if (e < N3AB) {
+                if (c0 < NCD) X[c0 * PX + e] = Tc(j > 0 ? d0 + (double)X[c0 * PX + e] : d0);
+                if (c0 + 1 < NCD) X[(c0 + 1) * PX + e] = Tc(j > 0 ? d1 + (double)X[(c0 + 1) * PX + e] : d1);
+              }
+            }
+          });
+        } else {
+          // ket transform: lane = bra Hermite index, every ket component (in
+          // chunks of kChunk components, R re-read per chunk)
+          for (int e = lane; e < N3AB; e += 32) {
+            const int base = tuvt[e];
+            wq::static_for<(NCD + wq::kChunk - 1) / wq::kChunk>([&](auto CH_) {
+              constexpr int c0 = decltype(CH_)::value * wq::kChunk;
+              constexpr int nc = NCD - c0 < wq::kChunk ? NCD - c0 : wq::kChunk;
+              Tc xa[nc];
+#pragma unroll
+              for (int k = 0; k < nc; ++k) xa[k] = Tc(0);
+              wq::static_for<N3CD>([&](auto F_) {
+                constexpr int f = decltype(F_)::value;
+                constexpr int ft = wq::tuv_t(f), fu = wq::tuv_u(f), fv = wq::tuv_v(f);
+                if constexpr (wq::chunk_uses(LC, LD, c0, nc, ft, fu, fv)) {
+                  const Tc r = R[base + (ft * BOX + fu) * BOX + fv];
+                  wq::static_for<nc>([&](auto K_) {
+                    constexpr int cd = c0 + decltype(K_)::value;
+                    if constexpr (wq::uses(LC, LD, cd, ft, fu, fv))
+                      xa[cd - c0] += Tk[wq::term_at(LC, LD, cd, ft, fu, fv)] * r;
+                  });
+                }
+              });
+              if constexpr (S::SPHR && !MMA) {
+                if (a.spherical) {  // one chunk holds all ket components: spherical rows of X
+                  Tc xs[S::FCD];
+                  sph_pair<LC, LD>(xa, xs);
+                  if (j > 0) {
+#pragma unroll
+                    for (int k = 0; k < S::FCD; ++k) xs[k] += X[k * PX + e];
+                  }
+#pragma unroll
+                  for (int k = 0; k < S::FCD; ++k) X[k * PX + e] = xs[k];
+                  return;
+                }
+              }
+              if (j > 0) {  // later ket primitives add to X
+#pragma unroll
+                for (int k = 0; k < nc; ++k) xa[k] += X[(c0 + k) * PX + e];
+              }
+#pragma unroll
+              for (int k = 0; k < nc; ++k) X[(c0 + k) * PX + e] = xa[k];
+            });
+          }
+        }
+        __syncwarp();
+      }
+      if constexpr (MMA) {
+        // bra product G[ab][cd] += sum_e E^ab[e] X[cd][e]: rows ab, columns
+        // cd, depth e; A the dense bra coefficient products, B from X, D in
+        // the lane's accumulators across the bra primitives.
+        const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+        for (int mt = 0; mt < S::MT3; ++mt) {
+          const int ab = mt * 8 + g;
+          const int pa = ab < NAB ? cmp_ab[ab] : 0;
+          double af[S::KT3];
+#pragma unroll
+          for (int kk = 0; kk < S::KT3; ++kk) {
+            const int e = kk * 4 + t4;
+            double v = 0.0;
+            if (ab < NAB && e < N3AB) {
+              const int pos = tuvt[e];
+              const int et = pos / (BOX * BOX), eu = (pos / BOX) % BOX, ev = pos % BOX;
+              v = (double)Eb[(pa & 1023) + et] * (double)Eb[((pa >> 10) & 1023) + eu] * (double)Eb[(pa >> 20) + ev];
+            }
+            af[kk] = v;
+          }
+#pragma unroll
+          for (int nt = 0; nt < S::NT; ++nt) {
+            const int cd = nt * 8 + g;
+#pragma unroll
+            for (int kk = 0; kk < S::KT3; ++kk) {
+              const int e = kk * 4 + t4;
+              const double bv = (cd < NCD && e < N3AB) ? (double)X[cd * PX + e] : 0.0;
+              wq::dmma(dacc[(mt * S::NT + nt) * 2], dacc[(mt * S::NT + nt) * 2 + 1], af[kk], bv);
+            }
+          }
+        }
+      } else if constexpr (S::MP) {
+        // bra transform into the lane's accumulators: lane = ket component
+        // (spherical ones when the ket transform produced them)
+        if (lane < ((S::SPHR && a.spherical) ? S::FCD : NCD)) {
+          wq::static_for<N3AB>([&](auto E_) {
+            constexpr int e = decltype(E_)::value;
+            constexpr int et = wq::tuv_t(e), eu = wq::tuv_u(e), ev = wq::tuv_v(e);
+            const Tc xv = X[lane * PX + e];
+            wq::static_for<NAB>([&](auto K_) {
+              constexpr int ab = decltype(K_)::value;
+              if constexpr (wq::uses(LA, LB, ab, et, eu, ev)) gacc[ab] += Tb[wq::term_at(LA, LB, ab, et, eu, ev)] * xv;
+            });
+          });
+        }
+      } else {
+        // bra transform: lane = ket component, every bra component (in chunks)
+        for (int cd = lane; cd < NCD; cd += 32) {
+          wq::static_for<(NAB + wq::kChunk - 1) / wq::kChunk>([&](auto CH_) {
+            constexpr int a0 = decltype(CH_)::value * wq::kChunk;
+            constexpr int na = NAB - a0 < wq::kChunk ? NAB - a0 : wq::kChunk;
+            Tc acc[na];
+#pragma unroll
+            for (int k = 0; k < na; ++k) acc[k] = Tc(0);
+            wq::static_for<N3AB>([&](auto E_) {
+              constexpr int e = decltype(E_)::value;
+              constexpr int et = wq::tuv_t(e), eu = wq::tuv_u(e), ev = wq::tuv_v(e);
+              if constexpr (wq::chunk_uses(LA, LB, a0, na, et, eu, ev)) {
+                const Tc xv = X[cd * PX + e];
+                wq::static_for<na>([&](auto K_) {
+                  constexpr int ab = a0 + decltype(K_)::value;
+                  if constexpr (wq::uses(LA, LB, ab, et, eu, ev))
+                    acc[ab - a0] += Tb[wq::term_at(LA, LB, ab, et, eu, ev)] * xv;
                 });
               }
             });
 #pragma unroll
-            for (int k = 0; k < nc; ++k) X[(c0 + k) * PX + e] = xa[k];
+            for (int k = 0; k < na; ++k) Gc[(a0 + k) * PG + cd] = (double)acc[k];
           });
         }
-        __syncwarp();
       }
-      // bra transform: lane = ket component, every bra component (in chunks)
-      for (int cd = lane; cd < NCD; cd += 32) {
-        wq::static_for<(NAB + wq::kChunk - 1) / wq::kChunk>([&](auto CH_) {
-          constexpr int a0 = decltype(CH_)::value * wq::kChunk;
-          constexpr int na = NAB - a0 < wq::kChunk ? NAB - a0 : wq::kChunk;
-          Tc acc[na];
+      __syncwarp();
+    }
+    if constexpr (MMA) {
+      // D fragments to the Cartesian block (R, in region A, is no longer needed)
+      const int g = lane >> 2, t4 = lane & 3;
 #pragma unroll
-          for (int k = 0; k < na; ++k) acc[k] = Tc(0);
-          wq::static_for<N3AB>([&](auto E_) {
-            constexpr int e = decltype(E_)::value;
-            constexpr int et = wq::tuv_t(e), eu = wq::tuv_u(e), ev = wq::tuv_v(e);
-            if constexpr (wq::chunk_uses(LA, LB, a0, na, et, eu, ev)) {
-              const Tc xv = X[cd * PX + e];
-              wq::static_for<na>([&](auto K_) {
-                constexpr int ab = a0 + decltype(K_)::value;
-                if constexpr (wq::uses(LA, LB, ab, et, eu, ev))
-                  acc[ab - a0] += Tb[wq::term_at(LA, LB, ab, et, eu, ev)] * xv;
-              });
-            }
-          });
+      for (int mt = 0; mt < S::MT3; ++mt)
 #pragma unroll
-          for (int k = 0; k < na; ++k) Gc[(a0 + k) * PG + cd] = (double)acc[k];
-        });
+        for (int nt = 0; nt < S::NT; ++nt) {
+          const int ab = mt * 8 + g, c0 = nt * 8 + 2 * t4;
+          if (ab < NAB) {
+            if (c0 < NCD) Gc[ab * PG + c0] = dacc[(mt * S::NT + nt) * 2];
+            if (c0 + 1 < NCD) Gc[ab * PG + c0 + 1] = dacc[(mt * S::NT + nt) * 2 + 1];
+          }
+        }
+      __syncwarp();
+    } else if constexpr (S::MP) {
+      // the accumulated block to shared memory (R, in region A, is no longer needed)
+      if (S::SPHR && a.spherical) {
+        if (lane < S::FCD) {
+          Tc gs[S::FAB];
+          sph_pair<LA, LB>(gacc, gs);
+#pragma unroll
+          for (int k = 0; k < S::FAB; ++k) Gc[k * PG + lane] = (double)gs[k];
+        }
+      } else if (lane < NCD) {
+#pragma unroll
+        for (int k = 0; k < NAB; ++k) Gc[k * PG + lane] = (double)gacc[k];
       }
       __syncwarp();
     }
     if (lane == 0) {
       cnt_q += 1;
-      cnt_p += 1;
+      cnt_p += (unsigned long long)nbp * nkp;
     }
     if (a.spherical)
-      wq_finish<LA, LB, LC, LD, Tc, true>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane);
+      wq_finish<LA, LB, LC, LD, Tc, true, S::SPHR && !MMA>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane);
     else
       wq_finish<LA, LB, LC, LD, Tc, false>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane);
     __syncwarp();

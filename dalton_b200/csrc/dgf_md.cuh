@@ -4,9 +4,70 @@
 // kernels.
 #pragma once
 
+#include <utility>
+
 #include "dgf_internal.h"
+#include "dgf_sph.h"
 
 namespace dgf {
+
+// Calls f(std::integral_constant<int, i>) for i = 0 .. N-1, so that the loop
+// index is a constant expression inside f (index arithmetic and term
+// selection at compile time).
+template <typename F, int... I>
+__device__ __forceinline__ void static_for_impl(F &&f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F &&f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// One index of the Cartesian -> spherical transform with compile-time
+// coefficients (zero ones drop out): for i < NI, spherical m < 2L+1, r < NR,
+//   out[(i * (2L+1) + m) * NR + r] = sum_{x < N} C_L[m][X0 + x] in[(i * N + x) * NR + r]
+// (X0 > 0: a chunk of the Cartesian components, the partial sums of which
+// add up across chunks).
+template <int L, int NI, int N, int X0, int NR, typename TI, typename TO>
+__device__ __forceinline__ void sph_index(const TI *in, TO *out) {
+  constexpr int M = 2 * L + 1;
+#pragma unroll
+  for (int i = 0; i < NI; ++i)
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      static_for<M>([&](auto M_) {
+        constexpr int m = decltype(M_)::value;
+        TO s = TO(0);
+        static_for<N>([&](auto X_) {
+          constexpr int x = decltype(X_)::value;
+          constexpr double c = sph::coef<L>(m, X0 + x);
+          if constexpr (c != 0.0) s += TO(c) * TO(in[(i * N + x) * NR + r]);
+        });
+        out[(i * M + m) * NR + r] = s;
+      });
+}
+
+// Both indices of a shell pair block in[ncart(L1)][ncart(L2)] to spherical
+// functions, out[F1][F2] (F = 2L+1 for L >= 2, ncart(L) for s and p).
+template <int L1, int L2, typename T>
+__device__ __forceinline__ void sph_pair(const T *in, T *out) {
+  constexpr int N1 = ncart(L1), N2 = ncart(L2);
+  constexpr int F1 = L1 >= 2 ? 2 * L1 + 1 : N1, F2 = L2 >= 2 ? 2 * L2 + 1 : N2;
+  T t[F1 * N2];
+  if constexpr (L1 >= 2) {
+    sph_index<L1, 1, N1, 0, N2>(in, t);
+  } else {
+#pragma unroll
+    for (int k = 0; k < N1 * N2; ++k) t[k] = in[k];
+  }
+  if constexpr (L2 >= 2) {
+    sph_index<L2, F1, N2, 0, 1>(t, out);
+  } else {
+#pragma unroll
+    for (int k = 0; k < F1 * F2; ++k) out[k] = t[k];
+  }
+}
+
 
 __host__ __device__ constexpr int nfun(int l, int spherical) { return (spherical && l >= 2) ? 2 * l + 1 : ncart(l); }
 

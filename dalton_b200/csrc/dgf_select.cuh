@@ -12,11 +12,18 @@ namespace dgf {
 // shape of SYMLOP's bound (DALTON/abacus/her2drv.F:2666-2692) with the
 // working-basis density.
 __device__ __forceinline__ double quartet_bound(const JKArgs &a, const PairRec &b, const PairRec &k) {
-  const float *dm = a.dmax;
-  const int n = a.nshell;
-  float dj = fmaxf(dm[b.shA * n + b.shB], dm[k.shA * n + k.shB]);
-  float dk = fmaxf(fmaxf(dm[b.shA * n + k.shA], dm[b.shA * n + k.shB]),
-                   fmaxf(dm[b.shB * n + k.shA], dm[b.shB * n + k.shB]));
+  float dj, dk;
+  if (a.dmax_w) {  // batches: shell-pair maxima at the shells' first functions in the molecule's block
+    const float *dm = a.dmax_w + k.dbase;
+    const int n = k.nbfm;
+    dj = fmaxf(dm[b.aoA * n + b.aoB], dm[k.aoA * n + k.aoB]);
+    dk = fmaxf(fmaxf(dm[b.aoA * n + k.aoA], dm[b.aoA * n + k.aoB]), fmaxf(dm[b.aoB * n + k.aoA], dm[b.aoB * n + k.aoB]));
+  } else {
+    const float *dm = a.dmax;
+    const int n = a.nshell;
+    dj = fmaxf(dm[b.shA * n + b.shB], dm[k.shA * n + k.shB]);
+    dk = fmaxf(fmaxf(dm[b.shA * n + k.shA], dm[b.shA * n + k.shB]), fmaxf(dm[b.shB * n + k.shA], dm[b.shB * n + k.shB]));
+  }
   return b.Q * k.Q * (double)fmaxf(4.0f * dj, dk);
 }
 
@@ -41,7 +48,7 @@ __device__ __forceinline__ int quartet_select(const JKArgs &a, const PairRec &b,
                                               const PairRec *kp) {
   if (b.Q * k.Q < a.schwarz_thr) return 3;
   if (a.blk_gab && block_bound(a, bp, kp) < a.dens_thr) return 2;
-  if (!a.dmax || a.mode == 0) return 0;
+  if ((!a.dmax && !a.dmax_w) || a.mode == 0) return 0;
   const double bound = quartet_bound(a, b, k);
   if (a.mode == 1 && bound < a.split) return 1;
   if (a.mode == 2 && bound >= a.split) return 1;

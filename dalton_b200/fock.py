@@ -75,8 +75,17 @@ class FockBuilder:
         return int(n.value)
 
     def copy_tuning_from(self, other: "FockBuilder"):
-        """Use the kernel choices ``other.autotune`` found."""
+        """Use the kernel choices (and mixed-form splits) ``other.autotune`` found."""
         _lib.check(self._lib.dgf_copy_tuning(self._h, other._h), "dgf_copy_tuning")
+
+    def set_class_kernel(self, cls, variant, precision=64):
+        """Pin the kernel of quartet class ``cls`` = (la, lb, lc, ld): variant
+        -4 warp per quartet with FP64 tensor-core (DMMA) transforms, -3 warp
+        per quartet, -2 warp team, -1 cooperative team, 0.. thread chunk
+        variants."""
+        la, lb, lc, ld = (int(x) for x in cls)
+        _lib.check(self._lib.dgf_set_class_kernel(self._h, la, lb, lc, ld, int(precision), int(variant)),
+                   "dgf_set_class_kernel")
 
     @staticmethod
     def _ifctyp(ifctyp, nd):

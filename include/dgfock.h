@@ -209,7 +209,8 @@ typedef struct {
   int32_t la, lb, lc, ld;   /* angular momenta of the class (ab|cd) */
   int32_t precision;        /* 64 = FP64, 32 = FP32 contraction */
   int32_t kernel;           /* 0 = thread-per-quartet, 1 = cooperative team, 2 = warp teams,
-                               4 = warp-per-quartet (single primitive pairs, L >= 4),
+                               4 = warp-per-quartet (L >= 4), 6 = warp-per-quartet with
+                               FP64 tensor-core (DMMA) transforms,
                                5 = two-electron gradient (dgf_grad2e*: quartets are the plan's,
                                primitive quartets estimated from the classes' mean primitive
                                pairs) */
@@ -229,8 +230,10 @@ int dgf_get_profile(const dgf_ctx *ctx, dgf_class_time *out, int max, int *count
 
 /* Batched Fock builds of many molecules (no counterpart in Dalton, which
  * builds one molecule per run): one launch per quartet class covers every
- * molecule's canonical quartet queue, merged class by class; the launch
- * sequence can be captured once as a CUDA graph and replayed.  Contexts must
+ * molecule's canonical quartet queue, merged class by class; the launches
+ * run on four streams forked from the caller's stream and joined back
+ * before the epilogue, and the sequence can be captured once as a CUDA
+ * graph and replayed.  Contexts must
  * live on one device with the same spherical flag and stay alive while the
  * batch exists.  Matrices are packed: molecule k's N_k x N_k block starts at
  * offsets[k] (offsets[nmol] = total doubles), see dgf_batch_layout. */
@@ -243,10 +246,11 @@ int dgf_batch_layout(const dgf_batch *batch, dgf_int *offsets /* nmol + 1 */);
  * pointers to packed D and F.  use_graph = 1: the first call captures the
  * launch sequence into a CUDA graph, later calls with the same pointers,
  * options and stream replay it.  `stream` is a cudaStream_t (NULL for the
- * legacy default stream).  Kernel choices per class come from the context
+ * legacy default stream).  Kernel choices per class, and with mixed_cutoff
+ * > 0 the classes split into FP64 and FP32 launches, come from the context
  * with the most basis functions at dgf_batch_create time (tune it with
- * dgf_autotune first).  Only the FP64 Schwarz-screened form (ifthrs >= 20,
- * mixed_cutoff = 0, one shard). */
+ * dgf_autotune first, with the same mixed_cutoff).  Schwarz-screened form
+ * only: ifthrs >= 16, one shard, hfxmu = 0. */
 int dgf_fock_batch(dgf_batch *batch, const double *dmat_packed_device, double *fmat_packed_device,
                    const dgf_options *opt, int use_graph, void *stream, dgf_stats *stats);
 
@@ -263,6 +267,15 @@ int dgf_autotune(dgf_ctx *ctx, const double *dmat_device, const dgf_options *opt
  * counterpart in Dalton), so that contexts of similar molecules share one
  * tuning run. */
 int dgf_copy_tuning(dgf_ctx *dst, const dgf_ctx *src);
+
+/* Pin the kernel of one quartet class (la lb|lc ld), as the autotuner would:
+ * precision 64 or 32; variant -4 warp per quartet with FP64 tensor-core
+ * (DMMA) transforms, -3 warp per quartet, -2 warp team, -1
+ * cooperative team, 0.. thread-kernel chunk variants.  Launches the chosen
+ * kernel cannot serve (e.g. a warp kernel restricted to one primitive pair
+ * per side) fall back to the default kernel.  DGF_ERR_UNSUPPORTED when the
+ * variant does not exist for the class. */
+int dgf_set_class_kernel(dgf_ctx *ctx, int la, int lb, int lc, int ld, int precision, int variant);
 
 /* Measurement helper (not part of the HERFCK contract): FP64 and FP32 FMA
  * throughput of device `device` in TFLOP/s from a register-resident FMA
