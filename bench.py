@@ -485,12 +485,14 @@ def alkane_leg(args, flush, fp64_peak, fp32_peak):
     setup_s = time.perf_counter() - t0
     D, H = core_guess_density(fb, mol)
     steps, warmup = max(2, min(args.steps, 3)), 1
-    ms_untuned, _ = timed_builds(fb, D, steps, warmup, flush)
+    ms_untuned, Fdef = timed_builds(fb, D, steps, warmup, flush)
+    Fdef = Fdef.clone()
     t0 = time.perf_counter()
     fb.autotune(D, thrs=THRS, mixed_cutoff=MIXED_CUTOFF)
     tune_s = time.perf_counter() - t0
     ms64, F64 = timed_builds(fb, D, steps, warmup, flush)
     F64 = F64.clone()
+    tuned_dF = float(torch.max(torch.abs(F64 - Fdef)))  # the tuned kernels against the default ones
     msmx, Fmx = timed_builds(fb, D, steps, warmup, flush, MIXED_CUTOFF)
     dE = abs(0.5 * float(torch.sum(D * (Fmx - F64))))
     quartets = fb.ao_quartets(THRS)
@@ -499,6 +501,7 @@ def alkane_leg(args, flush, fp64_peak, fp32_peak):
            "fp64_ms_default_kernels": ms_untuned, "autotune_s": tune_s, "context_s": setup_s,
            "fp64_ms": ms64, "mixed_ms": msmx, "speedup_mixed_vs_fp64": ms64 / msmx,
            "mixed_energy_error_Eh": dE, "mixed_max_abs_dF": float(torch.max(torch.abs(Fmx - F64))),
+           "tuned_vs_default_kernels_max_abs_dF": tuned_dF,
            "quartets": quartets, "quartets_per_s_fp64": quartets / (ms64 * 1e-3),
            "quartets_per_s_mixed": quartets / (msmx * 1e-3),
            "top_kernel_fp64": top_kernel(fb, D, 0.0, fp64_peak, fp32_peak)}
@@ -566,6 +569,7 @@ def main():
     H = torch.tensor(T_np + V_np, device=dev)
     enuc = mol.nuclear_repulsion()
     # Per-class kernel choice on this density (FP64 and FP32 candidates, mixed split).
+    Fdef = build(D, False).clone()  # default kernels, to check the tuned choice against
     t0 = time.perf_counter()
     tuning = fb.autotune(D, thrs=THRS, mixed_cutoff=MIXED_CUTOFF)
     tune_s = time.perf_counter() - t0
@@ -585,6 +589,7 @@ def main():
     emx = float(0.5 * torch.sum(D * (2 * H + Fmx))) + enuc
     dE = abs(emx - e64)
     dF = float(torch.max(torch.abs(Fmx - F64)))
+    tuned_dF = float(torch.max(torch.abs(F64 - Fdef)))
     mixed_ok = dE <= 1e-6
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
@@ -758,7 +763,7 @@ def main():
             "run": {"mixed_cutoff": MIXED_CUTOFF, "parallelism": f"cost-weighted quartet-queue shards x{world}",
                     "l2": "flushed (256 MB write) before every timed step", "density": density_source},
             "fp64": {"ms": ms64, "quartets_per_s": quartets / (ms64 * 1e-3), "quartets": quartets,
-                     "working_basis_quartets": q64},
+                     "working_basis_quartets": q64, "tuned_vs_default_kernels_max_abs_dF": tuned_dF},
             "mixed": {"ms": msmx, "quartets_per_s": quartets / (msmx * 1e-3), "quartets": quartets,
                       "working_basis_quartets": qmx,
                       "energy_error_Eh": dE, "max_abs_dF": dF, "speedup_vs_fp64": ms64 / msmx},

@@ -53,8 +53,7 @@ struct GradBra {
 // Cartesian components: spherical blocks are mapped back with the transposed
 // Cartesian -> spherical tables, so that sum_sph G_sph I_sph = sum_cart G I.
 template <int LX, int LY, bool SPH>
-__device__ __forceinline__ void cart_block(const double *__restrict__ D, int N, int p0, int q0,
-                                           const double *sph, double *out) {
+__device__ __forceinline__ void cart_block(const double *__restrict__ D, int N, int p0, int q0, double *out) {
   constexpr int NX = ncart(LX), NY = ncart(LY);
   constexpr bool TX = SPH && LX >= 2, TY = SPH && LY >= 2;
   constexpr int FX = TX ? 2 * LX + 1 : NX, FY = TY ? 2 * LY + 1 : NY;
@@ -63,33 +62,40 @@ __device__ __forceinline__ void cart_block(const double *__restrict__ D, int N, 
   for (int x = 0; x < FX; ++x)
 #pragma unroll
     for (int y = 0; y < FY; ++y) f[x * FY + y] = D[(size_t)(p0 + x) * N + q0 + y];
+  // transposed tables with compile-time coefficients (zero ones drop out)
   double t1[NX * FY];
 #pragma unroll
-  for (int i = 0; i < NX; ++i)
-#pragma unroll
-    for (int y = 0; y < FY; ++y) {
+  for (int y = 0; y < FY; ++y)
+    static_for<NX>([&](auto I_) {
+      constexpr int i = decltype(I_)::value;
       if constexpr (TX) {
         double s = 0.0;
-#pragma unroll
-        for (int x = 0; x < FX; ++x) s += sph[sph_offset(LX) + x * NX + i] * f[x * FY + y];
+        static_for<FX>([&](auto X_) {
+          constexpr int x = decltype(X_)::value;
+          constexpr double c = sph::coef<LX>(x, i);
+          if constexpr (c != 0.0) s += c * f[x * FY + y];
+        });
         t1[i * FY + y] = s;
       } else {
         t1[i * FY + y] = f[i * FY + y];
       }
-    }
+    });
 #pragma unroll
   for (int i = 0; i < NX; ++i)
-#pragma unroll
-    for (int j = 0; j < NY; ++j) {
+    static_for<NY>([&](auto J_) {
+      constexpr int j = decltype(J_)::value;
       if constexpr (TY) {
         double s = 0.0;
-#pragma unroll
-        for (int y = 0; y < FY; ++y) s += t1[i * FY + y] * sph[sph_offset(LY) + y * NY + j];
+        static_for<FY>([&](auto Y_) {
+          constexpr int y = decltype(Y_)::value;
+          constexpr double c = sph::coef<LY>(y, j);
+          if constexpr (c != 0.0) s += t1[i * FY + y] * c;
+        });
         out[i * NY + j] = s;
       } else {
         out[i * NY + j] = t1[i * FY + j];
       }
-    }
+    });
 }
 
 // Chunks of the ket's Cartesian (c, d) components a launch is split into
@@ -99,7 +105,7 @@ constexpr int grad_chunks(int LA, int LB, int LC, int LD) { return (LA + LB + LC
 
 // Chunk CH of CDN handles the ket components cd = c ND + d in [CD0, CD1).
 template <int LA, int LB, int LC, int LD, bool SPH, int CDN, int CH>
-__device__ __forceinline__ void grad_body(const JKArgs &a, const double *tab, const double *sph, double *bt,
+__device__ __forceinline__ void grad_body(const JKArgs &a, const double *tab, double *bt,
                                           double *gsh) {
   constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -157,20 +163,20 @@ __device__ __forceinline__ void grad_body(const JKArgs &a, const double *tab, co
       if (a.same_class && ib == ic + a.ket_off) w *= 0.5;
       // G_abcd = w [2 (D1_ab D2_cd + D2_ab D1_cd) - hfx/2 (D1_ac D2_bd + D2_ac D1_bd + D1_ad D2_bc + D2_ad D1_bc)]
       double ab1[NA * NB], ab2[NA * NB], cd1[NCD], cd2[NCD];
-      cart_block<LA, LB, SPH>(a.G1, N, br.aoA, br.aoB, sph, ab1);
-      cart_block<LA, LB, SPH>(a.G2, N, br.aoA, br.aoB, sph, ab2);
-      cart_block<LC, LD, SPH>(a.G1, N, kt.aoA, kt.aoB, sph, cd1);
-      cart_block<LC, LD, SPH>(a.G2, N, kt.aoA, kt.aoB, sph, cd2);
+      cart_block<LA, LB, SPH>(a.G1, N, br.aoA, br.aoB, ab1);
+      cart_block<LA, LB, SPH>(a.G2, N, br.aoA, br.aoB, ab2);
+      cart_block<LC, LD, SPH>(a.G1, N, kt.aoA, kt.aoB, cd1);
+      cart_block<LC, LD, SPH>(a.G2, N, kt.aoA, kt.aoB, cd2);
 #pragma unroll
       for (int x = 0; x < NA * NB; ++x)
 #pragma unroll
         for (int y = CD0; y < CD1; ++y) G[x * NCDc + y - CD0] = 2.0 * w * (ab1[x] * cd2[y] + ab2[x] * cd1[y]);
       if (h != 0.0) {
         double ac1[NA * NC], ac2[NA * NC], bd1[NB * ND], bd2[NB * ND];
-        cart_block<LA, LC, SPH>(a.G1, N, br.aoA, kt.aoA, sph, ac1);
-        cart_block<LA, LC, SPH>(a.G2, N, br.aoA, kt.aoA, sph, ac2);
-        cart_block<LB, LD, SPH>(a.G1, N, br.aoB, kt.aoB, sph, bd1);
-        cart_block<LB, LD, SPH>(a.G2, N, br.aoB, kt.aoB, sph, bd2);
+        cart_block<LA, LC, SPH>(a.G1, N, br.aoA, kt.aoA, ac1);
+        cart_block<LA, LC, SPH>(a.G2, N, br.aoA, kt.aoA, ac2);
+        cart_block<LB, LD, SPH>(a.G1, N, br.aoB, kt.aoB, bd1);
+        cart_block<LB, LD, SPH>(a.G2, N, br.aoB, kt.aoB, bd2);
 #pragma unroll
         for (int i = 0; i < NA; ++i)
 #pragma unroll
@@ -184,10 +190,10 @@ __device__ __forceinline__ void grad_body(const JKArgs &a, const double *tab, co
                     w * h * (ac1[i * NC + k] * bd2[j * ND + l] + ac2[i * NC + k] * bd1[j * ND + l]);
               }
         double ad1[NA * ND], ad2[NA * ND], bc1[NB * NC], bc2[NB * NC];
-        cart_block<LA, LD, SPH>(a.G1, N, br.aoA, kt.aoB, sph, ad1);
-        cart_block<LA, LD, SPH>(a.G2, N, br.aoA, kt.aoB, sph, ad2);
-        cart_block<LB, LC, SPH>(a.G1, N, br.aoB, kt.aoA, sph, bc1);
-        cart_block<LB, LC, SPH>(a.G2, N, br.aoB, kt.aoA, sph, bc2);
+        cart_block<LA, LD, SPH>(a.G1, N, br.aoA, kt.aoB, ad1);
+        cart_block<LA, LD, SPH>(a.G2, N, br.aoA, kt.aoB, ad2);
+        cart_block<LB, LC, SPH>(a.G1, N, br.aoB, kt.aoA, bc1);
+        cart_block<LB, LC, SPH>(a.G2, N, br.aoB, kt.aoA, bc2);
 #pragma unroll
         for (int i = 0; i < NA; ++i)
 #pragma unroll
@@ -417,13 +423,13 @@ __device__ __forceinline__ void grad_body(const JKArgs &a, const double *tab, co
 // One thread per quartet, 32 consecutive quartets of the class queue per
 // warp; SPH selects the spherical (1) or Cartesian (0) density blocks.
 template <int LA, int LB, int LC, int LD, bool SPH, int CDN, int CH>
-__device__ __forceinline__ void grad_dispatch(int chunk, const JKArgs &a, const double *tab, const double *sph,
-                                              double *bt, double *gsh) {
+__device__ __forceinline__ void grad_dispatch(int chunk, const JKArgs &a, const double *tab, double *bt,
+                                              double *gsh) {
   if constexpr (CH < CDN) {
     if (chunk == CH)
-      grad_body<LA, LB, LC, LD, SPH, CDN, CH>(a, tab, sph, bt, gsh);
+      grad_body<LA, LB, LC, LD, SPH, CDN, CH>(a, tab, bt, gsh);
     else
-      grad_dispatch<LA, LB, LC, LD, SPH, CDN, CH + 1>(chunk, a, tab, sph, bt, gsh);
+      grad_dispatch<LA, LB, LC, LD, SPH, CDN, CH + 1>(chunk, a, tab, bt, gsh);
   }
 }
 
@@ -432,16 +438,14 @@ __global__ void __launch_bounds__(kGradBlock) grad_thread_kernel(const JKArgs a)
   constexpr int CDN = grad_chunks(LA, LB, LC, LD);
   using S = GradBra<LA, LB>;
   __shared__ double tab[kBoysTableDoubles];
-  __shared__ double sph[kSphTableDoubles];
   __shared__ double bt_all[kGradWarps][S::kSize];
   __shared__ double gsh_all[3 * kGradSmemAtoms];
   const bool smem_acc = a.natom <= kGradSmemAtoms;
   for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
-  for (int i = threadIdx.x; i < kSphTableDoubles; i += blockDim.x) sph[i] = a.sph[i];
   if (smem_acc)
     for (int i = threadIdx.x; i < 3 * a.natom; i += blockDim.x) gsh_all[i] = 0.0;
   __syncthreads();
-  grad_dispatch<LA, LB, LC, LD, SPH, CDN, 0>(blockIdx.y, a, tab, sph, bt_all[threadIdx.x >> 5],
+  grad_dispatch<LA, LB, LC, LD, SPH, CDN, 0>(blockIdx.y, a, tab, bt_all[threadIdx.x >> 5],
                                              smem_acc ? gsh_all : nullptr);
   if (smem_acc) {
     __syncthreads();

@@ -6,8 +6,9 @@
 // Each warp of a block works through its own contiguous range of the class
 // queue, one quartet at a time; every index pattern is known at compile
 // time and the lanes split the work of each step:
-//   R_tuv            Hermite recursion level by level in a (L+1)^3 box in
-//                    shared memory, one (t,u,v) per lane     (HERI, her2her.F)
+//   R_tuv            Hermite recursion level by level in a box in shared
+//                    memory (strides chosen per class against bank
+//                    conflicts), one (t,u,v) per lane        (HERI, her2her.F)
 //   X[cd][tuv]       ket transform, one bra Hermite index tuv per lane: each
 //                    R value is read once and applied to every ket
 //                    component that uses it, with the ket's Hermite
@@ -107,10 +108,60 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 
 using ::dgf::static_for;
 
+// Layout of the R box: R_tuv at position SA t + SB u + v (t + u + v <= L).
+// The lanes of the ket transform read R at (t,u,v) + (tau,nu,phi) for the
+// bra Hermite indices, and the recursion writes one level at a time; the
+// strides are chosen per class so that those reads (8-byte values, one
+// 16-lane half of the warp per wavefront) fall in distinct banks as far as
+// possible, without enlarging the box beyond (L+1)^3.
+struct BoxStrides {
+  int sa, sb;
+};
+// Wavefronts of the 16-lane halves reading the positions of Hermite indices
+// 0 .. n3(m)-1 (tuv_index order).
+constexpr int box_waves(int sa, int sb, int m) {
+  int tot = 0, k = 0, mx = 0;
+  int cnt[16] = {};
+  for (int s = 0; s <= m; ++s)
+    for (int t = s; t >= 0; --t)
+      for (int u = s - t; u >= 0; --u) {
+        const int b = (sa * t + sb * u + (s - t - u)) % 16;
+        if (++cnt[b] > mx) mx = cnt[b];
+        if (++k == 16) {
+          tot += mx;
+          k = mx = 0;
+          for (int i = 0; i < 16; ++i) cnt[i] = 0;
+        }
+      }
+  return tot + mx;
+}
+constexpr int box_cost(int sa, int sb, int L, int LAB, int LCD) {
+  int c = n3(LCD) * box_waves(sa, sb, LAB);  // ket transform: one read per ket Hermite index
+  for (int m = 1; m <= L; ++m) c += 3 * box_waves(sa, sb, m);  // recursion levels
+  return c;
+}
+constexpr BoxStrides box_strides(int L, int LAB, int LCD) {
+  const int box = L + 1;
+  BoxStrides best{box * box, box};
+  int bc = box_cost(best.sa, best.sb, L, LAB, LCD);
+  for (int b = L + 1; b < L + 9; ++b)
+    for (int a = L * b + 1; a < L * b + 25; ++a) {
+      if (a * L + 1 > box * box * box) continue;
+      const int c = box_cost(a, b, L, LAB, LCD);
+      if (c < bc) {
+        bc = c;
+        best = BoxStrides{a, b};
+      }
+    }
+  return best;
+}
+
 // Per-warp shared memory of class (LA LB | LC LD) in units of 8 bytes.
 template <int LA, int LB, int LC, int LD, typename Tc>
 struct Shape {
   static constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD, BOX = L + 1;
+  static constexpr BoxStrides BS = box_strides(L, LAB, LCD);
+  static constexpr int SA = BS.sa, SB = BS.sb, RBOX = SA * L + 1;  // R box strides and size
   static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   static constexpr int NAB = NA * NB, NCD = NC * ND, N3AB = n3(LAB), N3CD = n3(LCD), N3L = n3(L);
   static constexpr int EA = (LA + 1) * (LB + 1) * (LAB + 1), EC = (LC + 1) * (LD + 1) * (LCD + 1);
@@ -121,7 +172,7 @@ struct Shape {
   static constexpr int FCm = cmax(NC, LC >= 2 ? 2 * LC + 1 : NC), FDm = cmax(ND, LD >= 2 ? 2 * LD + 1 : ND);
   static constexpr int W = sizeof(Tc) == 8 ? 1 : 2;  // Tc values per 8-byte unit
   // region A: the two R boxes, later the Cartesian (ab|cd) block and the final block
-  static constexpr int RA = cmax((2 * BOX * BOX * BOX + W - 1) / W, NAB * PG);
+  static constexpr int RA = cmax((2 * RBOX + W - 1) / W, NAB * PG);
   // region B: X, later the block with spherical bra functions
   static constexpr int RB = cmax((NCD * PX + W - 1) / W, NAB * PG);
   // Hermite 1D tables and product tables of bra and ket (Tc)
@@ -384,7 +435,7 @@ template <int LA, int LB, int LC, int LD, typename Tc, bool MMA>
 __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
   using S = wq::Shape<LA, LB, LC, LD, Tc>;
   static_assert(!MMA || S::MMA_OK, "DMMA form of a class it does not fit");
-  constexpr int L = S::L, BOX = S::BOX, NAB = S::NAB, NCD = S::NCD, N3AB = S::N3AB,
+  constexpr int L = S::L, SA = S::SA, SB = S::SB, NAB = S::NAB, NCD = S::NCD, N3AB = S::N3AB,
                 N3CD = S::N3CD, N3L = S::N3L, EA = S::EA, EC = S::EC, PX = S::PX, PG = S::PG;
   extern __shared__ double sm[];
   double *tab = sm;
@@ -397,7 +448,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
   double *regA = wbase, *regB = regA + S::RA;
   Tc *Eb = (Tc *)(regB + S::RB), *Ek = Eb + 3 * EA, *Tb = Ek + 3 * EC, *Tk = Tb + S::TAB;
   double *Db = regB + S::RB + S::RT;
-  Tc *R0 = (Tc *)regA, *R1 = R0 + BOX * BOX * BOX;
+  Tc *R0 = (Tc *)regA, *R1 = R0 + S::RBOX;
   Tc *X = (Tc *)regB;
   double *Gc = regA, *Gs = regB;
 
@@ -406,7 +457,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
   for (int e = threadIdx.x; e < N3L; e += blockDim.x) {
     int t, u, v;
     tuv_decode(e, t, u, v);
-    tuvt[e] = (t * BOX + u) * BOX + v;  // position of (t,u,v) in the R box
+    tuvt[e] = t * SA + u * SB + v;  // position of (t,u,v) in the R box
   }
   if constexpr (MMA) {
     wq_comp_index<LA, LB>(cmp_ab, threadIdx.x, blockDim.x);
@@ -512,16 +563,16 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
           const int cnt = n3(L - n);
           for (int e = lane; e < cnt; e += 32) {
             const int pos = tuvt[e];
-            const int t = pos / (BOX * BOX), u = (pos / BOX) % BOX, v = pos % BOX;
+            const int t = pos / SA, u = (pos % SA) / SB, v = (pos % SA) % SB;
             Tc val;
             if (e == 0) {
               val = Tc(Fs[n]);
             } else if (t > 0) {
-              val = tx * prev[pos - BOX * BOX];
-              if (t > 1) val += Tc(t - 1) * prev[pos - 2 * BOX * BOX];
+              val = tx * prev[pos - SA];
+              if (t > 1) val += Tc(t - 1) * prev[pos - 2 * SA];
             } else if (u > 0) {
-              val = ty * prev[pos - BOX];
-              if (u > 1) val += Tc(u - 1) * prev[pos - 2 * BOX];
+              val = ty * prev[pos - SB];
+              if (u > 1) val += Tc(u - 1) * prev[pos - 2 * SB];
             } else {
               val = tz * prev[pos - 1];
               if (v > 1) val += Tc(v - 1) * prev[pos - 2];
@@ -550,7 +601,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
               double v = 0.0;
               if (cd < NCD && f < N3CD) {
                 const int pos = tuvt[f];
-                const int ft = pos / (BOX * BOX), fu = (pos / BOX) % BOX, fv = pos % BOX;
+                const int ft = pos / SA, fu = (pos % SA) / SB, fv = (pos % SA) % SB;
                 v = (double)Ek[(pc & 1023) + ft] * (double)Ek[((pc >> 10) & 1023) + fu] * (double)Ek[(pc >> 20) + fv];
               }
               bf[kk] = v;
@@ -588,7 +639,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
                 constexpr int f = decltype(F_)::value;
                 constexpr int ft = wq::tuv_t(f), fu = wq::tuv_u(f), fv = wq::tuv_v(f);
                 if constexpr (wq::chunk_uses(LC, LD, c0, nc, ft, fu, fv)) {
-                  const Tc r = R[base + (ft * BOX + fu) * BOX + fv];
+                  const Tc r = R[base + ft * SA + fu * SB + fv];
                   wq::static_for<nc>([&](auto K_) {
                     constexpr int cd = c0 + decltype(K_)::value;
                     if constexpr (wq::uses(LC, LD, cd, ft, fu, fv))
@@ -636,7 +687,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
             double v = 0.0;
             if (ab < NAB && e < N3AB) {
               const int pos = tuvt[e];
-              const int et = pos / (BOX * BOX), eu = (pos / BOX) % BOX, ev = pos % BOX;
+              const int et = pos / SA, eu = (pos % SA) / SB, ev = (pos % SA) % SB;
               v = (double)Eb[(pa & 1023) + et] * (double)Eb[((pa >> 10) & 1023) + eu] * (double)Eb[(pa >> 20) + ev];
             }
             af[kk] = v;

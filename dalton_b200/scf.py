@@ -86,9 +86,11 @@ def rhf(bs: BasisSet, fb: FockBuilder | None = None, conv: float = 1e-8, maxiter
         nbuild += 1
         G_prev, D_prev = G, D
         F = H + G
-        energy = float(0.5 * torch.sum(D * (H + F))) + enuc
         err = X.T @ (F @ D @ S - S @ D @ F) @ X
-        en = float(torch.linalg.norm(err))
+        # the iteration's one device-to-host read: energy and error norm together
+        e_and_norm = torch.stack([0.5 * torch.sum(D * (H + F)), torch.linalg.norm(err)]).cpu()
+        energy = float(e_and_norm[0]) + enuc
+        en = float(e_and_norm[1])
         history.append((energy, en, bool(full)))
         if ifthrs_schedule:  # next build's screening threshold (sirdiis.F:1224-1248, DIFDEN form)
             ithrs = int(-np.log10(max(en, 1e-300) / scrfac)) + 3
