@@ -22,7 +22,8 @@ EXPORTS = ["dgf_default_options", "dgf_create", "dgf_destroy", "dgf_fock", "dgf_
            "dgf_grad2e_device", "dgf_grad2e_bilinear_device", "dgf_oneint", "dgf_grad1e", "dgf_set_profiling", "dgf_get_profile",
            "dgf_measure_fma_peak", "dgf_autotune", "dgf_info", "dgf_strerror", "dgf_last_error",
            "dgf_batch_create", "dgf_batch_destroy", "dgf_batch_layout", "dgf_fock_batch",
-           "dgf_fock_device_noalloc", "dgf_count_ao_quartets", "dgf_copy_tuning", "dgf_set_class_kernel"]
+           "dgf_fock_device_noalloc", "dgf_count_ao_quartets", "dgf_copy_tuning", "dgf_set_class_kernel",
+           "dgf_store_integrals", "dgf_fock_stored", "dgf_store_release"]
 
 
 class DgfBasis(ctypes.Structure):
@@ -92,6 +93,9 @@ def load() -> ctypes.CDLL:
     lib.dgf_count_ao_quartets.argtypes = [vp, ctypes.c_double, _ip]
     lib.dgf_copy_tuning.argtypes = [vp, vp]
     lib.dgf_set_class_kernel.argtypes = [vp] + [ctypes.c_int] * 6
+    lib.dgf_store_integrals.argtypes = [vp, ctypes.c_double, ctypes.c_int64, vp, ctypes.POINTER(ctypes.c_int64)]
+    lib.dgf_fock_stored.argtypes = [vp, dgf_int, _ip, vp, vp, ctypes.POINTER(DgfOptions), vp, ctypes.POINTER(DgfStats)]
+    lib.dgf_store_release.argtypes = [vp]
     lib.dgf_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dgf_get_profile.argtypes = [vp, ctypes.POINTER(DgfClassTime), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.dgf_measure_fma_peak.argtypes = [ctypes.c_int, _dp, _dp]

@@ -136,7 +136,8 @@ static void free_ctx(dgf_ctx *c) {
   cudaSetDevice(c->device);
   void *ptrs[] = {c->d_pairs, c->d_pp,     c->d_boys,   c->d_sph,   c->d_D,     c->d_Ds,    c->d_Fh, c->d_io,
                   c->d_dmax,  c->d_cnt,    c->d_qoff,   c->d_wmap_i, c->d_wmap_c, c->d_wmeta, c->d_wdims, c->d_gw,
-                  c->d_shinfo, c->d_blk_gab, c->d_blk_info, c->d_blk_dmax, c->d_ks_i, c->d_ks_q, c->d_ks_pp};
+                  c->d_shinfo, c->d_blk_gab, c->d_blk_info, c->d_blk_dmax, c->d_ks_i, c->d_ks_q, c->d_ks_pp,
+                  c->d_store};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1082,11 +1083,25 @@ static void shard_range(const dgf_ctx *c, size_t e, int64_t r, int64_t n, int64_
   *q1 = cut(r + 1);
 }
 
+// Values of one quartet's integral block of class pair (X, Y) in the store.
+static int64_t store_nint(const dgf_ctx *c, int X, int Y) {
+  const int la = cls_l1(X), lb = X - la * (la + 1) / 2, lc = cls_l1(Y), ld = Y - lc * (lc + 1) / 2;
+  return (int64_t)nfun(la, c->spherical) * nfun(lb, c->spherical) * nfun(lc, c->spherical) * nfun(ld, c->spherical);
+}
+
+// stored = true: the conventional form, digesting the blocks of the integral
+// store (dgf_store_integrals) instead of evaluating integrals.
 static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double *dmat_dev, double *fmat_dev,
-                     const dgf_options *opt, cudaStream_t st, dgf_stats *stats) {
+                     const dgf_options *opt, cudaStream_t st, dgf_stats *stats, bool stored = false) {
   dgf_options o;
   dgf_default_options(&o);
   if (opt) o = *opt;
+  if (stored) {
+    if (!c->d_store) DGF_FAIL(DGF_ERR_ARG, "no integral store: call dgf_store_integrals first");
+    if (o.thrs != c->store_thrs) DGF_FAIL(DGF_ERR_ARG, "the integral store was made for another Schwarz threshold");
+    if (o.mixed_cutoff > 0.0 || o.hfxmu != 0.0)
+      DGF_FAIL(DGF_ERR_UNSUPPORTED, "stored integrals are FP64 1/r12 integrals: no mixed form, no range separation");
+  }
   if (!(o.thrs >= 0.0)) DGF_FAIL(DGF_ERR_ARG, "thrs must be >= 0");
   if (o.shard_count <= 0) o.shard_count = 1;
   if (o.shard_index < 0 || o.shard_index >= o.shard_count) DGF_FAIL(DGF_ERR_ARG, "shard_index out of range");
@@ -1240,6 +1255,18 @@ static int fock_impl(dgf_ctx *c, int ndmat, const dgf_int *ifctyp, const double 
         const bool split = o.mixed_cutoff > 0.0 && c->split_ok[cp.X][cp.Y] &&
                            select_kernel(c, cp.X, cp.Y, 1, cp.bucket == 0).launch != nullptr;
         const int Lq = la + lb + lc + ld;
+        if (stored) {  // conventional form: digest the stored blocks
+          a.store_in = c->d_store;
+          a.store_base = c->store_off[e];
+          a.store_nint = (int)store_nint(c, cp.X, cp.Y);
+          a.mode = 0;
+          a.counters = c->d_cnt + 4 * (nlaunch_class % kCounterSlots);
+          ++nlaunch_class;
+          int r = launch_kernel(c, jk_stored_kernel(cp.X, cp.Y), cp.X, cp.Y, a, st, 0);
+          if (r) return r;
+          ++launches;
+          continue;
+        }
         for (int part = 0; part < (split ? 2 : 1); ++part) {
           a.mode = split ? 1 + part : 0;
           // the FP32 half reads the low-degree Boys table
@@ -1305,6 +1332,110 @@ extern "C" int dgf_fock_device(dgf_ctx *c, dgf_int ndmat, const dgf_int *ifctyp,
   if (r || ndmat == 0) return r;
   DeviceGuard g(c->device);
   return fock_impl(c, (int)ndmat, ifctyp, dmat_device, fmat_device, opt, (cudaStream_t)stream, stats);
+}
+
+// An integral kernel that writes whole blocks: the tuned choice unless it is
+// a thread kernel split into A-component chunks, else a one-chunk thread
+// variant, else the warp-per-quartet kernel, else the cooperative one.
+static const ClassKernel &store_kernel(const dgf_ctx *c, int X, int Y, bool ket1) {
+  const bool bra1 = c->cls_max_npp[X] == 1;
+  const ClassKernel &t = jk_kernel_variant(X, Y, 0, c->choice[X][Y][0], ket1, bra1);
+  if (t.launch && (t.kind != kKindThread || t.chunks == 1)) return t;
+  for (int v = 0; v < kThreadVariants; ++v) {
+    const ClassKernel &k = jk_kernel_variant(X, Y, 0, v, ket1, bra1);
+    if (k.launch && k.chunks == 1) return k;
+  }
+  const ClassKernel &w = jk_kernel_variant(X, Y, 0, -3, ket1, bra1);
+  if (w.launch) return w;
+  return jk_kernel_variant(X, Y, 0, -1, ket1, bra1);
+}
+
+extern "C" int dgf_store_integrals(dgf_ctx *c, double thrs, int64_t max_bytes, void *stream, int64_t *bytes) {
+  if (!c) DGF_FAIL(DGF_ERR_ARG, "ctx is NULL");
+  if (!(thrs >= 0.0)) DGF_FAIL(DGF_ERR_ARG, "thrs must be >= 0");
+  DeviceGuard g(c->device);
+  int r = build_plan(c, thrs);
+  if (r) return r;
+  std::vector<int64_t> off(c->plan.size());
+  int64_t tot = 0;
+  for (size_t e = 0; e < c->plan.size(); ++e) {
+    off[e] = tot;
+    tot += c->plan[e].nquartet * store_nint(c, c->plan[e].X, c->plan[e].Y);
+  }
+  if (bytes) *bytes = tot * 8;
+  if (max_bytes > 0 && tot * 8 > max_bytes)
+    DGF_FAIL(DGF_ERR_NOMEM, "the integral store needs " + std::to_string(tot * 8) + " bytes, more than max_bytes");
+  if (c->d_store) cudaFree(c->d_store);
+  c->d_store = nullptr;
+  c->store_doubles = 0;
+  c->store_thrs = -1.0;
+  if (dev_alloc(&c->d_store, (size_t)std::max<int64_t>(tot, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    c->d_store = nullptr;
+    DGF_FAIL(DGF_ERR_NOMEM, "device allocation of the integral store (" + std::to_string(tot * 8) + " bytes) failed");
+  }
+  r = ensure_slots(c, 1);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  JKArgs a = base_args(c);
+  a.nslot = 1;
+  a.D = c->d_D;
+  a.Ds = c->d_Ds;
+  a.Fh = c->d_Fh;
+  a.schwarz_thr = thrs;
+  a.store_out = c->d_store;
+  const int saved_prof = c->profiling;
+  c->profiling = 0;
+  for (size_t e = 0; e < c->plan.size(); ++e) {
+    const ClassPlan &cp = c->plan[e];
+    if (cp.nquartet <= 0) continue;
+    a.bra = c->d_pairs + c->cls_off[cp.X];
+    a.ket = c->d_pairs + c->cls_off[cp.Y] + cp.kb0;
+    a.ket_off = cp.kb0;
+    a.ket_pp0 = ket_pp0_of(c, cp);
+    set_ket_table(c, cp, a);
+    a.nbra = c->cls_off[cp.X + 1] - c->cls_off[cp.X];
+    a.same_class = (cp.X == cp.Y);
+    a.qoff = c->d_qoff + cp.off;
+    a.q_begin = 0;
+    a.nquartet = cp.nquartet;
+    const int Lq = cls_l1(cp.X) + (cp.X - cls_l1(cp.X) * (cls_l1(cp.X) + 1) / 2) + cls_l1(cp.Y) +
+                   (cp.Y - cls_l1(cp.Y) * (cls_l1(cp.Y) + 1) / 2);
+    a.boys = c->d_boys + (size_t)Lq * kBoysTableDoubles;
+    a.store_base = off[e];
+    a.store_nint = (int)store_nint(c, cp.X, cp.Y);
+    a.counters = c->d_cnt;
+    r = launch_kernel(c, store_kernel(c, cp.X, cp.Y, cp.bucket == 0), cp.X, cp.Y, a, st, 0);
+    if (r) {
+      c->profiling = saved_prof;
+      return r;
+    }
+  }
+  c->profiling = saved_prof;
+  DGF_CUDA_CHECK(cudaGetLastError());
+  c->store_off.swap(off);
+  c->store_doubles = tot;
+  c->store_thrs = thrs;
+  return DGF_OK;
+}
+
+extern "C" int dgf_store_release(dgf_ctx *c) {
+  if (!c) DGF_FAIL(DGF_ERR_ARG, "ctx is NULL");
+  DeviceGuard g(c->device);
+  if (c->d_store) cudaFree(c->d_store);
+  c->d_store = nullptr;
+  c->store_doubles = 0;
+  c->store_thrs = -1.0;
+  c->store_off.clear();
+  return DGF_OK;
+}
+
+extern "C" int dgf_fock_stored(dgf_ctx *c, dgf_int ndmat, const dgf_int *ifctyp, const double *dmat_device,
+                               double *fmat_device, const dgf_options *opt, void *stream, dgf_stats *stats) {
+  int r = check_fock_args(c, ndmat, ifctyp, dmat_device, fmat_device);
+  if (r || ndmat == 0) return r;
+  DeviceGuard g(c->device);
+  return fock_impl(c, (int)ndmat, ifctyp, dmat_device, fmat_device, opt, (cudaStream_t)stream, stats, true);
 }
 
 extern "C" int dgf_fock(dgf_ctx *c, dgf_int ndmat, const dgf_int *ifctyp, const double *dmat, double *fmat,

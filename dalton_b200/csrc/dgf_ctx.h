@@ -58,6 +58,13 @@ struct dgf_ctx {
   int *d_wdims = nullptr;       // {nwf, nbf, 0, 0}
   double *d_gw = nullptr;       // working-basis densities of the two-electron gradient (2 nwf^2)
   int *d_shinfo = nullptr;      // per working shell: first function | function count (density bounds)
+  // conventional form: the integral store (dgf_store_integrals) for the plan
+  // of store_thrs, one block of store_nint(X, Y) values per quartet, plan
+  // entry e starting at store_off[e]
+  double *d_store = nullptr;
+  int64_t store_doubles = 0;
+  double store_thrs = -1.0;
+  std::vector<int64_t> store_off;
   std::vector<dgf::PairRec> pairs;  // class-major, Schwarz-descending inside a class
   int cls_off[dgf::kNumPairClass + 1] = {0};
   // per class: bucket boundaries (relative to the class start), pairs sorted by (bucket, -Schwarz bin, shells)

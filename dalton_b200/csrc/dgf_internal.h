@@ -124,6 +124,15 @@ struct JKArgs {
   double split;             // precision split bound
   double schwarz_thr;       // skip quartets with Q_AB Q_CD below this (0: the plan is exact)
   double erf_mu2;           // > 0: the attenuated operator erf(mu r12)/r12 with mu^2 = erf_mu2; 0: 1/r12
+  // conventional (stored-integral) form: store_out non-null makes the
+  // integral kernels write each evaluated quartet's block (layout [a][b][c][d],
+  // spherical or Cartesian functions, store_nint values) to store_out +
+  // store_base + q store_nint instead of digesting it; the digest kernels
+  // read the blocks from store_in the same way
+  double *store_out;
+  const double *store_in;
+  int64_t store_base;
+  int store_nint;
   int mode;                 // 0: all, 1: bound >= split only, 2: bound < split only
   double *diag_out;         // Schwarz mode: sqrt(max |(ab|ab)|) per bra pair, no digestion
   unsigned long long *counters;  // [0] quartets done, [1] primitive quartets, [2] skipped
@@ -186,6 +195,8 @@ constexpr int kThreadVariants = 2;
 // use their single-ket-primitive form); bra1: so do all pairs of the bra
 // class (with ket1, the condition of the warp-per-quartet kernel).
 const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1 = false, bool bra1 = false);
+// Digestion kernel of stored integral blocks of class pair (X, Y).
+const ClassKernel &jk_stored_kernel(int X, int Y);
 // variant -3 = warp-per-quartet kernel, -2 = warp-team kernel, -1 = team
 // kernel, >= 0 = thread-kernel variant (precision 0/1).
 const ClassKernel &jk_kernel_variant(int X, int Y, int precision, int variant, bool ket1 = false,

@@ -44,6 +44,8 @@ const ClassKernel &jk_kernel(int X, int Y, int precision, bool ket1, bool bra1) 
   return precision == 1 ? kNone : e.team;
 }
 
+const ClassKernel &jk_stored_kernel(int X, int Y) { return g_jk_table[X][Y].stored; }
+
 cudaError_t jk_prepare_all() {
   for (int X = 0; X < kNumPairClass; ++X)
     for (int Y = 0; Y <= X; ++Y)

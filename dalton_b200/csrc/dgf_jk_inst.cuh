@@ -20,6 +20,7 @@ struct JKEntry {
   ClassKernel warp[2];                   // warp-per-quartet kernel [FP64, FP32]
   bool warp_mp;                          // the warp kernel loops over primitive pairs (else one per side only)
   ClassKernel warp_mma;                  // warp-per-quartet kernel with DMMA transforms (FP64, any pairs)
+  ClassKernel stored;                    // digestion of stored integral blocks (conventional form)
   cudaError_t (*prepare[3])();           // one per generated part
 };
 

@@ -1,10 +1,12 @@
 // Instantiation of part 0 of the quartet-class kernel table (see
-// dgf_jk_inst.cuh): the cooperative, warp-team and warp-per-quartet kernels.
+// dgf_jk_inst.cuh): the cooperative, warp-team and warp-per-quartet kernels,
+// and the digestion kernel of stored integrals.
 #pragma once
 
 #include "dgf_jk_inst.cuh"
 #include "dgf_jk_team.cuh"
 #include "dgf_jk_warp.cuh"
+#include "dgf_jk_stored.cuh"
 
 namespace dgf {
 namespace jkinst {
@@ -46,6 +48,19 @@ cudaError_t prepare_warp() {
                               (int)W::smem(W::WPB));
 }
 
+template <int LA, int LB, int LC, int LD>
+void launch_stored_thread(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
+  jk_stored_thread_kernel<LA, LB, LC, LD><<<grid, block, smem, s>>>(a);
+}
+template <int LA, int LB, int LC, int LD>
+void launch_stored_warp(const JKArgs &a, int grid, int block, size_t smem, cudaStream_t s) {
+  jk_stored_warp_kernel<LA, LB, LC, LD><<<grid, block, smem, s>>>(a);
+}
+template <int LA, int LB, int LC, int LD>
+constexpr bool stored_by_thread() {
+  return ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) <= kStoredThreadMax;
+}
+
 template <int X, int Y>
 cudaError_t prepare_team() {
   constexpr int LA = cls_la(X), LB = cls_lb(X), LC = cls_la(Y), LD = cls_lb(Y);
@@ -61,6 +76,12 @@ cudaError_t prepare_team() {
     if (e == cudaSuccess) e = prepare_warp<LA, LB, LC, LD, float>();
     if constexpr (wq::Shape<LA, LB, LC, LD, double>::MMA_OK)
       if (e == cudaSuccess) e = prepare_warp<LA, LB, LC, LD, double, true>();
+  }
+  if constexpr (!stored_by_thread<LA, LB, LC, LD>()) {
+    using SS = StoredShape<LA, LB, LC, LD>;
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(jk_stored_warp_kernel<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)SS::smem(SS::WPB));
   }
   return e;
 }
@@ -82,6 +103,12 @@ void fill_team() {
     e.warp[1] = warp_entry<LA, LB, LC, LD, float>();
     e.warp_mp = wq::Shape<LA, LB, LC, LD, double>::MP && wq::Shape<LA, LB, LC, LD, float>::MP;
     if constexpr (wq::Shape<LA, LB, LC, LD, double>::MMA_OK) e.warp_mma = warp_entry<LA, LB, LC, LD, double, true>();
+  }
+  if constexpr (stored_by_thread<LA, LB, LC, LD>()) {
+    e.stored = ClassKernel{&launch_stored_thread<LA, LB, LC, LD>, kThreadBlock, 0, 1, kThreadBlock, kKindThread};
+  } else {
+    using SS = StoredShape<LA, LB, LC, LD>;
+    e.stored = ClassKernel{&launch_stored_warp<LA, LB, LC, LD>, 32 * SS::WPB, SS::smem(SS::WPB), 1, SS::WPB, kKindWarp};
   }
 }
 

@@ -267,6 +267,11 @@ __global__ void __launch_bounds__(128) jk_team_kernel(const JKArgs a) {
       }
     }
 
+    if (a.store_out) {  // conventional form: the block to the store
+      double *o = a.store_out + a.store_base + q * a.store_nint;
+      for (int e = tid; e < FA * FB * FC * FD; e += nt) o[e] = res[e];
+      continue;
+    }
     if (a.diag_out) {
       if (tid == 0) {
         double mx = 0.0;

@@ -475,6 +475,21 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
         for (int k = 0; k < ABC1 * FDc; ++k) g[k] = tmp[k];
       }
     }
+    // Conventional form: the block goes to the store (the host launches only
+    // one-chunk variants here, so g holds the whole block).
+    if (a.store_out) {
+      if (work) {
+        double *o = a.store_out + a.store_base + q * a.store_nint;
+        if (sphr) {
+#pragma unroll
+          for (int k = 0; k < FAc * FBc * FCc * FDc; ++k) o[k] = g[k];
+        } else {
+#pragma unroll
+          for (int k = 0; k < NACC; ++k) o[k] = g[k];
+        }
+      }
+      continue;
+    }
     // Digestion with compile-time function counts (spherical or Cartesian).
     if (!__any_sync(full, work)) continue;
     if (sphr)

@@ -247,7 +247,7 @@ __device__ __forceinline__ void sph_pass(const double *in, double *out, const do
 template <int LA, int LB, int LC, int LD, typename Tc, bool SPH, bool PRE = false>
 __device__ __forceinline__ void wq_finish(const JKArgs &a, double *Gc, double *Gs, double *Db,
                                           const double *sph, const PairRec &br, const PairRec &kt, int ib, int ic,
-                                          double w, int lane) {
+                                          double w, int lane, int64_t q) {
   using S = wq::Shape<LA, LB, LC, LD, Tc>;
   constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, PG = S::PG;
   constexpr int FA = (SPH && LA >= 2) ? 2 * LA + 1 : NA, FB = (SPH && LB >= 2) ? 2 * LB + 1 : NB;
@@ -280,6 +280,11 @@ __device__ __forceinline__ void wq_finish(const JKArgs &a, double *Gc, double *G
       double *t = src; src = dst; dst = t;
     }
     G = src;
+  }
+  if (a.store_out) {  // conventional form: the block to the store
+    double *o = a.store_out + a.store_base + q * a.store_nint;
+    for (int e = lane; e < FAB * FCD; e += 32) o[e] = G[(e / FCD) * PG + e % FCD];
+    return;
   }
   // Largest integral for the per-density Coulomb/exchange screen (ICEDIF).
   bool ice = false;
@@ -779,9 +784,9 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(const JKArgs a) {
       cnt_p += (unsigned long long)nbp * nkp;
     }
     if (a.spherical)
-      wq_finish<LA, LB, LC, LD, Tc, true, S::SPHR && !MMA>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane);
+      wq_finish<LA, LB, LC, LD, Tc, true, S::SPHR && !MMA>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane, q);
     else
-      wq_finish<LA, LB, LC, LD, Tc, false>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane);
+      wq_finish<LA, LB, LC, LD, Tc, false>(a, Gc, Gs, Db, sph, br, kt, ib, ic, w, lane, q);
     __syncwarp();
   }
   if (lane == 0 && a.counters) {

@@ -144,6 +144,49 @@ class FockBuilder:
             self.last_stats = st.as_dict()
         return fmat
 
+    def store_integrals(self, thrs=1e-12, max_bytes=0, stream=None):
+        """Conventional form: evaluate the integral blocks of every quartet of
+        the plan for ``thrs`` once and keep them in device memory (Dalton's
+        AOTWOINT file, held on the GPU).  Returns the store's size in bytes."""
+        import torch
+
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
+        nbytes = ctypes.c_int64()
+        _lib.check(self._lib.dgf_store_integrals(self._h, float(thrs), int(max_bytes), ctypes.c_void_p(stream),
+                                                 ctypes.byref(nbytes)), "dgf_store_integrals")
+        return nbytes.value
+
+    def release_store(self):
+        _lib.check(self._lib.dgf_store_release(self._h), "dgf_store_release")
+
+    def herfck_stored(self, dmat, fmat=None, ifctyp=13, hfxfac=1.0, thrs=1e-12, ifthrs=20, stream=None, stats=True,
+                      shard=(0, 1), icedif=3):
+        """HERFCK from the integral store (Dalton's SIRFCK2 over AOTWOINT):
+        ``dmat`` a CUDA float64 tensor (N,N) or (ndmat,N,N); same results as
+        ``herfck_device`` with the store's Schwarz threshold."""
+        import torch
+
+        if dmat.device.type != "cuda" or dmat.dtype != torch.float64:
+            raise ValueError("dmat must be a CUDA float64 tensor")
+        d = dmat.contiguous()
+        nd = 1 if d.dim() == 2 else d.shape[0]
+        if fmat is None:
+            fmat = torch.empty_like(d)
+        ift = self._ifctyp(ifctyp, nd)
+        opt = _lib.default_options(thrs=float(thrs), ifthrs=int(ifthrs), hfxfac=float(hfxfac),
+                                   shard_index=int(shard[0]), shard_count=int(shard[1]), icedif=int(icedif))
+        if stream is None:
+            stream = torch.cuda.current_stream(d.device).cuda_stream
+        st = _lib.DgfStats()
+        _lib.check(self._lib.dgf_fock_stored(self._h, nd, ift.ctypes.data_as(ctypes.POINTER(_lib.dgf_int)),
+                                             ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(fmat.data_ptr()),
+                                             ctypes.byref(opt), ctypes.c_void_p(stream),
+                                             ctypes.byref(st) if stats else None), "dgf_fock_stored")
+        if stats:
+            self.last_stats = st.as_dict()
+        return fmat
+
     def autotune(self, dmat, thrs=1e-12, hfxfac=1.0, mixed_cutoff=0.0):
         """Time every candidate kernel per quartet class on this density (a
         CUDA float64 tensor) and keep the fastest; with ``mixed_cutoff`` > 0

@@ -37,8 +37,10 @@ from .fock import FockBuilder
 def rhf(bs: BasisSet, fb: FockBuilder | None = None, conv: float = 1e-8, maxiter: int = 50, thrs: float = 1e-12,
         mixed_cutoff: float = 0.0, incremental: bool = True, full_every: int = 8, diis_size: int = 8,
         device: str = "cuda", verbose: bool = False, fixed_iterations: int | None = None,
-        ifthrs_schedule: bool = False):
-    """Run RHF; returns a dict with energy, density, orbitals, timings."""
+        ifthrs_schedule: bool = False, stored: bool = False):
+    """Run RHF; returns a dict with energy, density, orbitals, timings.
+    ``stored``: Fock builds from the builder's integral store (the
+    conventional form; ``fb.store_integrals(thrs)`` first)."""
     import torch
 
     fb = fb or FockBuilder(bs)
@@ -75,11 +77,14 @@ def rhf(bs: BasisSet, fb: FockBuilder | None = None, conv: float = 1e-8, maxiter
     for it in range(1, maxiter + 1):
         full = (not incremental) or G_prev is None or (it % full_every == 0) or newthr
         t0 = time.perf_counter()
-        if full:
-            G = fb.herfck_device(D, ifctyp=13, thrs=thrs, ifthrs=ifthrs, mixed_cutoff=mixed_cutoff)
+        if stored:
+            build = lambda dm: fb.herfck_stored(dm, ifctyp=13, thrs=thrs, ifthrs=ifthrs)
         else:
-            dG = fb.herfck_device(D - D_prev, ifctyp=13, thrs=thrs, ifthrs=ifthrs, mixed_cutoff=mixed_cutoff)
-            G = G_prev + dG
+            build = lambda dm: fb.herfck_device(dm, ifctyp=13, thrs=thrs, ifthrs=ifthrs, mixed_cutoff=mixed_cutoff)
+        if full:
+            G = build(D)
+        else:
+            G = G_prev + build(D - D_prev)
         ifthrs_used.append(ifthrs)
         torch.cuda.synchronize(dev)
         fock_ms += (time.perf_counter() - t0) * 1e3

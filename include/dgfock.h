@@ -228,6 +228,23 @@ int dgf_set_profiling(dgf_ctx *ctx, int on);
 /* Copy up to `max` records of the last profiled call; *count = records. */
 int dgf_get_profile(const dgf_ctx *ctx, dgf_class_time *out, int max, int *count);
 
+/* Conventional (stored-integral) form: Dalton's SIRFCK2 path over the
+ * AOTWOINT integral file (DALTON/sirius/sirfck.F:1122-1342), with the file
+ * held in device memory.  dgf_store_integrals evaluates the integral block
+ * of every quartet of the plan for Schwarz threshold thrs once (spherical or
+ * Cartesian functions as the basis, FP64, 1/r12) and keeps them on the
+ * device; *bytes receives the store's size (also on DGF_ERR_NOMEM, so that a
+ * caller can size max_bytes; max_bytes <= 0 means no limit besides the
+ * device).  dgf_fock_stored then builds Fock matrices as dgf_fock_device
+ * does (any IFCTYP codes, HFXFAC, IFTHRS/ICEDIF screening, shards) by
+ * digesting the stored blocks; its opt->thrs must equal the store's thrs,
+ * mixed_cutoff must be 0 and hfxmu 0.  A store made before a change of the
+ * context's tuning stays valid.  dgf_store_release frees it. */
+int dgf_store_integrals(dgf_ctx *ctx, double thrs, int64_t max_bytes, void *stream, int64_t *bytes);
+int dgf_fock_stored(dgf_ctx *ctx, dgf_int ndmat, const dgf_int *ifctyp, const double *dmat_device,
+                    double *fmat_device, const dgf_options *opt, void *stream, dgf_stats *stats);
+int dgf_store_release(dgf_ctx *ctx);
+
 /* Batched Fock builds of many molecules (no counterpart in Dalton, which
  * builds one molecule per run): one launch per quartet class covers every
  * molecule's canonical quartet queue, merged class by class; the launches
