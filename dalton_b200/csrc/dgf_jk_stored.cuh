@@ -73,10 +73,11 @@ __global__ void __launch_bounds__(kThreadBlock, 2) jk_stored_thread_kernel(const
 #pragma unroll
     for (int k = 0; k < NOUT; ++k) g[k] = (work && k < nint) ? __ldg(s + k) : 0.0;
     if (!__any_sync(full, work)) continue;
+    double jnone[1];
     if (a.spherical)
-      jk_digest<FA, FB, FC, FD>(a, g, work, ib, ic, ib0, br, kt, 0);
+      jk_digest<FA, FB, FC, FD, 1>(a, g, work, ib, ic, ib0, br, kt, 0, jnone, false);
     else
-      jk_digest<NA, NB, NC, ND>(a, g, work, ib, ic, ib0, br, kt, 0);
+      jk_digest<NA, NB, NC, ND, 1>(a, g, work, ib, ic, ib0, br, kt, 0, jnone, false);
     cnt_q += work ? 1 : 0;
   }
   if (a.counters) {

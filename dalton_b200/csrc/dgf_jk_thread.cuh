@@ -44,6 +44,87 @@ __device__ __forceinline__ void seg_end(int key, int lane, bool &head, int &end)
   end = after ? __ffs(after) - 2 : 31;
 }
 
+// K_ac/K_bc runs with at most kSegMaxValues values per lane are summed
+// before their atomics; from kSegRowsMin values on, through shared memory.
+constexpr int kSegMaxValues = 18;
+constexpr int kSegRowsMin = 8;
+constexpr int kSegStride = 33;  // doubles per row of a warp's buffer (32 lanes + 1 against bank conflicts)
+
+// Run sums of the group lanes' K_ac / K_bc values, which the lanes wrote as
+// columns of sbuf (row e < FA FC: K_ac[x][c], e = x FC + c; after that
+// K_bc[y][c]).  Lane e < NV sums row e over each run of lanes with the same
+// C shell and adds the total to the group bra's row; the run bounds, the
+// C shell and whether the run belongs to the group are warp-uniform.
+// Called by the whole warp; returns with sbuf free for reuse.
+template <int FA, int FC, int NV>
+__device__ __forceinline__ void seg_rows(double *sbuf, bool grp, int cfun, int send, double *Fg, const PairRec &brg,
+                                         int a_off) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  unsigned ends = __ballot_sync(full, send == lane);
+  const unsigned gmask = __ballot_sync(full, grp);
+  const double *row = sbuf + lane * kSegStride;
+  int row_f, col_f;  // this lane's row of F (function) and offset within the C shell
+  if (lane < FA * FC) {
+    row_f = brg.aoA + a_off + lane / FC;
+    col_f = lane % FC;
+  } else {
+    row_f = brg.aoB + (lane - FA * FC) / FC;
+    col_f = (lane - FA * FC) % FC;
+  }
+  int j0 = 0;
+  while (ends) {
+    const int j1 = __ffs(ends) - 1;
+    ends &= ends - 1;
+    const int cj = __shfl_sync(full, cfun, j1);
+    if ((gmask >> j1) & 1u) {
+      double r = 0.0;
+      if (lane < NV)
+        for (int j = j0; j <= j1; ++j) r += row[j];
+      if (lane < NV && r != 0.0) atomicAdd(Fg + (size_t)row_f * brg.nbfm + cj + col_f, r);
+    }
+    j0 = j1 + 1;
+  }
+  __syncwarp();
+}
+
+// One block of the digestion: s_o = sum_i g[gi(o, i)] d(i) for o < NO,
+// i < NI, each density value d(i) loaded once (repeated loads of the same
+// element are not merged across the atomics in between).  With NI <= NO
+// the NI values are held and each s_o is emitted as it is formed; otherwise
+// the NO sums accumulate over the loads.  emit(o, s) is called for every o
+// in order by every lane (s = 0 where !on), after the block's loads.
+template <int NO, int NI, typename GI, typename DV, typename EMIT>
+__device__ __forceinline__ void block_sums(bool on, const double *g, GI gi, DV dv, EMIT emit) {
+  if constexpr (NI <= NO) {
+    double d[NI];
+#pragma unroll
+    for (int i = 0; i < NI; ++i) d[i] = on ? dv(i) : 0.0;
+#pragma unroll
+    for (int o = 0; o < NO; ++o) {
+      double s = 0.0;
+#pragma unroll
+      for (int i = 0; i < NI; ++i) s += g[gi(o, i)] * d[i];
+      emit(o, s);
+    }
+  } else {
+    double s[NO];
+#pragma unroll
+    for (int o = 0; o < NO; ++o) s[o] = 0.0;
+    if (on) {
+#pragma unroll
+      for (int i = 0; i < NI; ++i) {
+        const double d = dv(i);
+#pragma unroll
+        for (int o = 0; o < NO; ++o) s[o] += g[gi(o, i)] * d;
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < NO; ++o) emit(o, s[o]);
+  }
+}
+
 // Digestion of one quartet block g[FA][FB][FC][FD] (FA rows of A starting at
 // function a_off) into the half Fock matrices with FP64 atomics: the six J/K
 // blocks of FCKCON (DALTON/abacus/herfckcon.F:66-80)
@@ -59,11 +140,22 @@ __device__ __forceinline__ void seg_end(int key, int lane, bool &head, int &end)
 // its Coulomb part of density k when max(|D|_AB,|D|_CD) max|g| < ice_thr
 // (bit 1 of icedif) and its exchange part when the exchange blocks' bound
 // does (bit 2), with the block maxima of the AO density.
-template <int FA, int FB, int FC, int FD>
+//
+// With jon (one density slot), the group lanes add their J_ab terms to the
+// registers jacc instead, which the caller reduces across the warp once the
+// warp leaves that bra (jk_jab_flush).
+//
+// With sbuf (the warp's kSegStride x 32 doubles of shared memory) and 8 to
+// 18 K_ac/K_bc values per lane, the runs are summed through shared memory
+// instead of shuffles: each lane writes its values as one column, then lane
+// e sums row e over each run and adds the run's total (seg_rows).
+template <int FA, int FB, int FC, int FD, int JN>
 __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool work, int ib, int ic, int gib,
-                                          const PairRec &br, const PairRec &kt, int a_off) {
+                                          const PairRec &br, const PairRec &kt, int a_off, double (&jacc)[JN],
+                                          bool jon, double *sbuf = nullptr) {
   // Segmented reduction of K_ac and K_bc where it is cheap next to the atomics it saves.
-  constexpr bool SEG = (FA + FB) * FC <= 18;
+  constexpr int NV = (FA + FB) * FC;
+  constexpr bool SEG = NV <= kSegMaxValues;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   double w = 0.0;
@@ -80,6 +172,13 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
   bool head = true;
   int send = lane;
   if (SEG) seg_end(grp ? kt.aoA : -1 - lane, lane, head, send);
+  // Shared-memory run sums pay a fixed scan of the warp's 32 columns plus
+  // one step per run; shuffles pay per value.  The buffer is used when the
+  // group's runs are few next to the values (measured: many short runs, as
+  // in (ps|ps), make the scan slower than the shuffles).
+  bool tseg = false;
+  if (SEG && NV >= kSegRowsMin && sbuf != nullptr)
+    tseg = 2 * __popc(__ballot_sync(full, grp && head)) <= NV;
   double aomax = 0.0;
   bool ice = false;
   if (a.ice_thr > 0.0 && work) {
@@ -97,9 +196,11 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
     const double *Dsk = a.Ds + k * a.slot_stride + db;
     double *Fk = a.Fh + k * a.slot_stride + db;
     double *Fg = a.Fh + k * a.slot_stride + brg.dbase;
-    // Rows of the bra's functions in D.
-    auto dA = [&](int x, int col) -> double { return Dk[(size_t)(br.aoA + a_off + x) * N + col]; };
-    auto dB = [&](int y, int col) -> double { return Dk[(size_t)(br.aoB + y) * N + col]; };
+    // Rows of the bra's functions in D.  D and Ds are read-only during the
+    // build, so their gathers take the non-coherent path and stay in
+    // registers across the atomics into Fh.
+    auto dA = [&](int x, int col) -> double { return __ldg(Dk + (size_t)(br.aoA + a_off + x) * N + col); };
+    auto dB = [&](int y, int col) -> double { return __ldg(Dk + (size_t)(br.aoB + y) * N + col); };
     double js = a.jscale[k] * w, ks = -a.kscale[k] * w;
     if (ice) {
       const int4 bb = block_of_pair(a.bra + ib), kb = block_of_pair(a.ket + ic);
@@ -112,119 +213,119 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
       if ((a.icedif & 2) && dk * aomax < a.ice_thr) ks = 0.0;
     }
     if (a.jscale[k] != 0.0) {
-      // J_ab: group lanes warp-reduced, others per lane
-#pragma unroll
-      for (int x = 0; x < FA; ++x)
-#pragma unroll
-        for (int y = 0; y < FB; ++y) {
-          double s = 0.0;
-          if (work && js != 0.0) {
-#pragma unroll
-            for (int c = 0; c < FC; ++c)
-#pragma unroll
-              for (int d = 0; d < FD; ++d)
-                s += g[((x * FB + y) * FC + c) * FD + d] * Dsk[(size_t)(kt.aoA + c) * N + kt.aoB + d];
+      const bool jw = work && js != 0.0;
+      // J_ab[x][y] = sum_cd g Ds_cd: group lanes warp-reduced (or held in
+      // jacc), others per lane
+      block_sums<FA * FB, FC * FD>(
+          jw, g, [&](int o, int i) { return o * FC * FD + i; },
+          [&](int i) { return __ldg(Dsk + (size_t)(kt.aoA + i / FD) * N + kt.aoB + i % FD); },
+          [&](int o, double s) {
+            const int x = o / FB, y = o % FB;
             s *= js;
-          }
-          double r = grp ? s : 0.0;
+            if constexpr (JN >= FA * FB) {
+              if (jon) {
+                if (grp) jacc[o] += s;
+                else if (work && s != 0.0) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + br.aoB + y, s);
+                return;
+              }
+            }
+            double r = grp ? s : 0.0;
 #pragma unroll
-          for (int off = 16; off > 0; off >>= 1) r += __shfl_xor_sync(full, r, off);
-          if (lane == 0 && r != 0.0) atomicAdd(Fg + (size_t)(brg.aoA + a_off + x) * brg.nbfm + brg.aoB + y, r);
-          if (work && !grp && s != 0.0) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + br.aoB + y, s);
-        }
-      // J_cd: per lane
-      if (work && js != 0.0) {
-#pragma unroll
-        for (int c = 0; c < FC; ++c)
-#pragma unroll
-          for (int d = 0; d < FD; ++d) {
-            double s = 0.0;
-#pragma unroll
-            for (int x = 0; x < FA; ++x)
-#pragma unroll
-              for (int y = 0; y < FB; ++y)
-                s += g[((x * FB + y) * FC + c) * FD + d] * Dsk[(size_t)(br.aoA + a_off + x) * N + br.aoB + y];
-            atomicAdd(Fk + (size_t)(kt.aoA + c) * N + kt.aoB + d, js * s);
-          }
-      }
+            for (int off = 16; off > 0; off >>= 1) r += __shfl_xor_sync(full, r, off);
+            if (lane == 0 && r != 0.0) atomicAdd(Fg + (size_t)(brg.aoA + a_off + x) * brg.nbfm + brg.aoB + y, r);
+            if (work && !grp && s != 0.0) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + br.aoB + y, s);
+          });
+      // J_cd[c][d] = sum_ab g Ds_ab: per lane
+      block_sums<FC * FD, FA * FB>(
+          jw, g, [&](int o, int i) { return i * FC * FD + o; },
+          [&](int i) { return __ldg(Dsk + (size_t)(br.aoA + a_off + i / FB) * N + br.aoB + i % FB); },
+          [&](int o, double s) {
+            if (jw) atomicAdd(Fk + (size_t)(kt.aoA + o / FD) * N + kt.aoB + o % FD, js * s);
+          });
     }
     if (a.kscale[k] != 0.0) {
       const bool kw = work && ks != 0.0;
-#pragma unroll
-      for (int x = 0; x < FA; ++x) {
-        // K_ac: runs of equal C reduced, the run's head adds
-#pragma unroll
-        for (int c = 0; c < FC; ++c) {
-          double s = 0.0;
-          if (kw) {
-#pragma unroll
-            for (int y = 0; y < FB; ++y)
-#pragma unroll
-              for (int d = 0; d < FD; ++d) s += g[((x * FB + y) * FC + c) * FD + d] * dB(y, kt.aoB + d);
+      // K_ac[x][c] = sum_yd g D_bd: runs of equal C reduced, the run's head adds
+      block_sums<FA * FC, FB * FD>(
+          kw, g, [&](int o, int i) { return (((o / FC) * FB + i / FD) * FC + o % FC) * FD + i % FD; },
+          [&](int i) { return dB(i / FD, kt.aoB + i % FD); },
+          [&](int o, double s) {
+            const int x = o / FC, c = o % FC;
             s *= ks;
-          }
-          if (SEG) {
-            const double r = seg_sum(grp ? s : 0.0, lane, send);
-            if (grp && head && r != 0.0) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, r);
-            if (kw && !grp) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, s);
-          } else if (kw) {
-            atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, s);
-          }
-        }
-        // K_ad: per lane
-#pragma unroll
-        for (int d = 0; d < FD; ++d) {
-          if (!kw) continue;
-          double s = 0.0;
-#pragma unroll
-          for (int y = 0; y < FB; ++y)
-#pragma unroll
-            for (int c = 0; c < FC; ++c) s += g[((x * FB + y) * FC + c) * FD + d] * dB(y, kt.aoA + c);
-          atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoB + d, ks * s);
-        }
-      }
-#pragma unroll
-      for (int y = 0; y < FB; ++y) {
-        // K_bc: runs of equal C reduced
-#pragma unroll
-        for (int c = 0; c < FC; ++c) {
-          double s = 0.0;
-          if (kw) {
-#pragma unroll
-            for (int x = 0; x < FA; ++x)
-#pragma unroll
-              for (int d = 0; d < FD; ++d) s += g[((x * FB + y) * FC + c) * FD + d] * dA(x, kt.aoB + d);
+            if (SEG && tseg) {
+              sbuf[o * kSegStride + lane] = grp ? s : 0.0;
+              if (kw && !grp) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, s);
+            } else if (SEG) {
+              const double r = seg_sum(grp ? s : 0.0, lane, send);
+              if (grp && head && r != 0.0) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, r);
+              if (kw && !grp) atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, s);
+            } else if (kw) {
+              atomicAdd(Fk + (size_t)(br.aoA + a_off + x) * N + kt.aoA + c, s);
+            }
+          });
+      // K_ad[x][d] = sum_yc g D_bc: per lane
+      block_sums<FA * FD, FB * FC>(
+          kw, g, [&](int o, int i) { return (((o / FD) * FB + i / FC) * FC + i % FC) * FD + o % FD; },
+          [&](int i) { return dB(i / FC, kt.aoA + i % FC); },
+          [&](int o, double s) {
+            if (kw) atomicAdd(Fk + (size_t)(br.aoA + a_off + o / FD) * N + kt.aoB + o % FD, ks * s);
+          });
+      // K_bc[y][c] = sum_xd g D_ad: runs of equal C reduced
+      block_sums<FB * FC, FA * FD>(
+          kw, g, [&](int o, int i) { return (((i / FD) * FB + o / FC) * FC + o % FC) * FD + i % FD; },
+          [&](int i) { return dA(i / FD, kt.aoB + i % FD); },
+          [&](int o, double s) {
+            const int y = o / FC, c = o % FC;
             s *= ks;
-          }
-          if (SEG) {
-            const double r = seg_sum(grp ? s : 0.0, lane, send);
-            if (grp && head && r != 0.0) atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, r);
-            if (kw && !grp) atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, s);
-          } else if (kw) {
-            atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, s);
-          }
-        }
-        // K_bd: per lane
-#pragma unroll
-        for (int d = 0; d < FD; ++d) {
-          if (!kw) continue;
-          double s = 0.0;
-#pragma unroll
-          for (int x = 0; x < FA; ++x)
-#pragma unroll
-            for (int c = 0; c < FC; ++c) s += g[((x * FB + y) * FC + c) * FD + d] * dA(x, kt.aoA + c);
-          atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoB + d, ks * s);
-        }
-      }
+            if (SEG && tseg) {
+              sbuf[(FA * FC + o) * kSegStride + lane] = grp ? s : 0.0;
+              if (kw && !grp) atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, s);
+            } else if (SEG) {
+              const double r = seg_sum(grp ? s : 0.0, lane, send);
+              if (grp && head && r != 0.0) atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, r);
+              if (kw && !grp) atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, s);
+            } else if (kw) {
+              atomicAdd(Fk + (size_t)(br.aoB + y) * N + kt.aoA + c, s);
+            }
+          });
+      // K_bd[y][d] = sum_xc g D_ac: per lane
+      block_sums<FB * FD, FA * FC>(
+          kw, g, [&](int o, int i) { return (((i / FC) * FB + o / FD) * FC + i % FC) * FD + o % FD; },
+          [&](int i) { return dA(i / FC, kt.aoA + i % FC); },
+          [&](int o, double s) {
+            if (kw) atomicAdd(Fk + (size_t)(br.aoB + o / FD) * N + kt.aoB + o % FD, ks * s);
+          });
+      if (SEG && tseg) seg_rows<FA, FC, NV>(sbuf, grp, grp ? kt.aoA : 0, send, Fg, brg, a_off);
     }
   }
+}
+
+// J_ab of bra pair jb held in the lanes' registers (slot 0, rows from
+// a_off): summed across the warp and added by lane 0, then cleared.  Called
+// by the whole warp.
+template <int FA, int FB, int JN>
+__device__ __forceinline__ void jk_jab_flush(const JKArgs &a, int jb, int a_off, double (&jacc)[JN]) {
+  if (jb < 0) return;
+  const PairRec bj = load_pair_fock(a.bra + jb);
+  double *F = a.Fh + bj.dbase;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int x = 0; x < FA; ++x)
+#pragma unroll
+    for (int y = 0; y < FB; ++y) {
+      double r = jacc[x * FB + y];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
+      if (lane == 0 && r != 0.0) atomicAdd(F + (size_t)(bj.aoA + a_off + x) * bj.nbfm + bj.aoB + y, r);
+      jacc[x * FB + y] = 0.0;
+    }
 }
 
 constexpr int kThreadBlock = 256;
 constexpr int kThreadWarps = kThreadBlock / 32;
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
-__device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, Tc *ebra,
+__device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, Tc *ebra, double *sbuf,
                                                unsigned long long &cnt_q, unsigned long long &cnt_p,
                                                unsigned long long &cnt_s) {
   constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD;
@@ -249,6 +350,15 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
   const int64_t bspan = ((nq + gridDim.x - 1) / gridDim.x + 31) & ~(int64_t)31;
   const int64_t bbegin = a.q_begin + (int64_t)blockIdx.x * bspan, bend = min(bbegin + bspan, a.nquartet);
   int ibw = -1;  // the warp's running bra
+  // J_ab of the warp's running bra accumulates in registers across its
+  // chunks (s and p bras, one density slot); one warp reduction per bra run.
+  constexpr bool JACC = !SPH_NEEDED && NAc * NB <= 9;
+  constexpr int JN = JACC ? NAc * NB : 1;
+  const bool jon = JACC && a.nslot == 1 && a.store_out == nullptr;
+  double jacc[JN];
+#pragma unroll
+  for (int e = 0; e < JN; ++e) jacc[e] = 0.0;
+  int jbra = -1;
   for (int64_t base = bbegin + (int64_t)warp * 32; base < bend; base += (int64_t)nw * 32) {
     const int64_t q = base + lane;
     const bool active = q < bend;
@@ -492,23 +602,46 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
     }
     // Digestion with compile-time function counts (spherical or Cartesian).
     if (!__any_sync(full, work)) continue;
+    if (JACC && jon && ib0 != jbra) {
+      jk_jab_flush<NAc, NB, JN>(a, jbra, A0, jacc);
+      jbra = ib0;
+    }
     if (sphr)
-      jk_digest<FAc, FBc, FCc, FDc>(a, g, work, ib, ic, ib0, br, kt, 0);
+      jk_digest<FAc, FBc, FCc, FDc, JN>(a, g, work, ib, ic, ib0, br, kt, 0, jacc, false, sbuf);
     else
-      jk_digest<NAc, NB, NC, ND>(a, g, work, ib, ic, ib0, br, kt, A0);
+      jk_digest<NAc, NB, NC, ND, JN>(a, g, work, ib, ic, ib0, br, kt, A0, jacc, jon, sbuf);
   }
+  if (JACC && jon) jk_jab_flush<NAc, NB, JN>(a, jbra, A0, jacc);
 }
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, const double *tab,
-                                                   Tc *ebra, unsigned long long &q, unsigned long long &p,
-                                                   unsigned long long &s) {
+                                                   Tc *ebra, double *sbuf, unsigned long long &q,
+                                                   unsigned long long &p, unsigned long long &s) {
   if constexpr (CH < CA) {
     if (chunk == CH)
-      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, ebra, q, p, s);
+      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, ebra, sbuf, q, p, s);
     else
-      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, ebra, q, p, s);
+      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, ebra, sbuf, q, p, s);
   }
+}
+
+// Rows of the shared-memory run buffer a class needs: the largest K_ac/K_bc
+// value count in [kSegRowsMin, kSegMaxValues] over its A chunks, spherical
+// and Cartesian (0: the class reduces its runs with shuffles only).
+template <int LA, int LB, int LC, int CA>
+constexpr int seg_rows_needed() {
+  constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC);
+  constexpr int FB = LB >= 2 ? 2 * LB + 1 : NB, FC = LC >= 2 ? 2 * LC + 1 : NC;
+  int best = 0;
+  for (int ch = 0; ch < CA; ++ch) {
+    const int nac = (ch + 1) * NA / CA - ch * NA / CA;
+    const int fa = LA >= 2 ? 2 * LA + 1 : nac;
+    const int nv[2] = {(nac + NB) * NC, (fa + FB) * FC};
+    for (int v : nv)
+      if (v >= kSegRowsMin && v <= kSegMaxValues && v > best) best = v;
+  }
+  return best;
 }
 
 // Resident blocks per SM the register allocation must allow: the low-L
@@ -529,13 +662,20 @@ template <int LA, int LB, int LC, int LD, typename Tc, int CA, int K1>
 __global__ void __launch_bounds__(kThreadBlock, thread_min_blocks(LA + LB + LC + LD))
     jk_thread_kernel(const JKArgs a) {
   constexpr int EA = (LA + 1) * (LB + 1) * (LA + LB + 1);
+  // The run buffer only where it fits the 48 KB of static shared memory
+  // beside the Boys table and the bra tables.
+  constexpr int SR0 = seg_rows_needed<LA, LB, LC, CA>();
+  constexpr int kOtherSmem = kBoysTableDoubles * 8 + kThreadWarps * 3 * EA * (int)sizeof(Tc);
+  constexpr int SR = (kOtherSmem + kThreadWarps * SR0 * kSegStride * 8 <= 48 * 1024 - 256) ? SR0 : 0;
   __shared__ double tab[kBoysTableDoubles];
   __shared__ Tc ebra_all[kThreadWarps][3 * EA];
+  __shared__ double segbuf[kThreadWarps][SR > 0 ? SR * kSegStride : 1];
   for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
   __syncthreads();
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
-  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, ebra_all[threadIdx.x >> 5], cnt_q, cnt_p,
-                                                cnt_s);
+  double *sbuf = SR > 0 ? segbuf[threadIdx.x >> 5] : nullptr;
+  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, ebra_all[threadIdx.x >> 5], sbuf, cnt_q,
+                                                cnt_p, cnt_s);
   if (a.counters) {
     const int lane = threadIdx.x & 31;
 #pragma unroll

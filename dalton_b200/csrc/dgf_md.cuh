@@ -123,12 +123,16 @@ __device__ __forceinline__ double poly_estrin(const double *__restrict__ c, doub
 // FP32 half of the mixed form (relative error ~2e-8, FP64 arithmetic).
 template <int M, int DEG = kBoysDeg>
 __device__ __forceinline__ void boys_eval(double T, const double *__restrict__ tab, double *F) {
+  // e^-T is formed once, ahead of the branch: the lanes of a warp often fall
+  // on both sides of kBoysTmax, and then both branches run.
+  double et = 0.0;
+  if (M > 0) et = exp(-T);
   if (T < kBoysTmax) {
     int i = (int)(T * kBoysPerUnit);
     double x = (T - (i + 0.5) * (1.0 / kBoysPerUnit)) * (2.0 * kBoysPerUnit);
     F[M] = poly_estrin<DEG>(tab + i * kBoysNcoef, x);
     if (M > 0) {
-      double et = exp(-T), t2 = 2.0 * T;
+      const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], et) * (1.0 / (2 * m + 1));
     }
@@ -136,7 +140,7 @@ __device__ __forceinline__ void boys_eval(double T, const double *__restrict__ t
     double rt = rsqrt(T);
     F[0] = 0.88622692545275801364908374167057 * rt;
     if (M > 0) {
-      double et = exp(-T), h = 0.5 * rt * rt;
+      const double h = 0.5 * rt * rt;
 #pragma unroll
       for (int m = 0; m < M; ++m) F[m + 1] = fma((double)(2 * m + 1), F[m], -et) * h;
     }
