@@ -326,7 +326,7 @@ constexpr int kThreadWarps = kThreadBlock / 32;
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *tab, Tc *ebra, double *sbuf,
-                                               unsigned long long &cnt_q, unsigned long long &cnt_p,
+                                               double *bsh, unsigned long long &cnt_q, unsigned long long &cnt_p,
                                                unsigned long long &cnt_s) {
   constexpr int L = LA + LB + LC + LD, LAB = LA + LB, LCD = LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -359,6 +359,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
 #pragma unroll
   for (int e = 0; e < JN; ++e) jacc[e] = 0.0;
   int jbra = -1;
+  int cbra = -1;  // single-primitive bra whose data and tables bsh / ebra hold
   for (int64_t base = bbegin + (int64_t)warp * 32; base < bend; base += (int64_t)nw * 32) {
     const int64_t q = base + lane;
     const bool active = q < bend;
@@ -441,17 +442,42 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
       const int ibl = __shfl_sync(full, ib, leader);
       const bool mine = work && ib == ibl && ((pending >> lane) & 1u);
       pending &= ~__ballot_sync(full, mine);
-      const PairRec brl = load_pair_fock(a.bra + ibl);
-      for (int i = 0; i < brl.npp; ++i) {
-        const PrimPair P1 = load_prim<true>(a.pp + brl.pp0 + i);
-        __syncwarp();
-        if (lane < 3) {
-          const Tc h1 = Tc(0.5 / P1.p);
-          const double pa = lane == 0 ? P1.PAx : lane == 1 ? P1.PAy : P1.PAz;
-          const double pb = lane == 0 ? P1.PBx : lane == 1 ? P1.PBy : P1.PBz;
-          herm_e<LA, LB, 1, Tc>(h1, Tc(pa), Tc(pb), ebra + lane * EA);
+      // The single-primitive bra the warp met last keeps its primitive data
+      // (p, P, K) and Hermite tables in the warp's shared memory, so a run of
+      // chunks on one bra loads and tabulates it once.
+      const bool cached = (ibl == cbra);
+      int npp = 1, pp0 = 0;
+      if (!cached) {
+        const PairRec brl = load_pair_fock(a.bra + ibl);
+        npp = brl.npp;
+        pp0 = brl.pp0;
+      }
+      for (int i = 0; i < npp; ++i) {
+        PrimPair P1;
+        if (!cached) {
+          P1 = load_prim<true>(a.pp + pp0 + i);
+          __syncwarp();
+          if (lane < 3) {
+            const Tc h1 = Tc(0.5 / P1.p);
+            const double pa = lane == 0 ? P1.PAx : lane == 1 ? P1.PAy : P1.PAz;
+            const double pb = lane == 0 ? P1.PBx : lane == 1 ? P1.PBy : P1.PBz;
+            herm_e<LA, LB, 1, Tc>(h1, Tc(pa), Tc(pb), ebra + lane * EA);
+          }
+          if (lane == 0) {
+            bsh[0] = P1.p;
+            bsh[1] = P1.Px;
+            bsh[2] = P1.Py;
+            bsh[3] = P1.Pz;
+            bsh[4] = P1.K;
+          }
+          __syncwarp();
+        } else {
+          P1.p = bsh[0];
+          P1.Px = bsh[1];
+          P1.Py = bsh[2];
+          P1.Pz = bsh[3];
+          P1.K = bsh[4];
         }
-        __syncwarp();
         if (!mine) continue;
         const Tc *ex1 = ebra, *ey1 = ebra + EA, *ez1 = ebra + 2 * EA;
         // One ket primitive pair (a zero K makes it contribute nothing).
@@ -545,6 +571,7 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
           }
         }
       }
+      cbra = (npp == 1) ? ibl : -1;
     }
     if (work) {
       cnt_q += (CH == 0);
@@ -616,13 +643,13 @@ __device__ __forceinline__ void jk_thread_body(const JKArgs &a, const double *ta
 
 template <int LA, int LB, int LC, int LD, typename Tc, int CA, int CH, int K1>
 __device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, const double *tab,
-                                                   Tc *ebra, double *sbuf, unsigned long long &q,
+                                                   Tc *ebra, double *sbuf, double *bsh, unsigned long long &q,
                                                    unsigned long long &p, unsigned long long &s) {
   if constexpr (CH < CA) {
     if (chunk == CH)
-      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, ebra, sbuf, q, p, s);
+      jk_thread_body<LA, LB, LC, LD, Tc, CA, CH, K1>(a, tab, ebra, sbuf, bsh, q, p, s);
     else
-      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, ebra, sbuf, q, p, s);
+      jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, CH + 1, K1>(chunk, a, tab, ebra, sbuf, bsh, q, p, s);
   }
 }
 
@@ -663,18 +690,26 @@ __global__ void __launch_bounds__(kThreadBlock, thread_min_blocks(LA + LB + LC +
     jk_thread_kernel(const JKArgs a) {
   constexpr int EA = (LA + 1) * (LB + 1) * (LA + LB + 1);
   // The run buffer only where it fits the 48 KB of static shared memory
-  // beside the Boys table and the bra tables.
+  // beside the Boys table and the bra tables, and only in classes that run
+  // one block per SM: two blocks with the buffer would not fit the small
+  // shared-memory carveout these kernels ask for (the rest of L1 caches the
+  // density gathers), which would halve their resident warps.
   constexpr int SR0 = seg_rows_needed<LA, LB, LC, CA>();
-  constexpr int kOtherSmem = kBoysTableDoubles * 8 + kThreadWarps * 3 * EA * (int)sizeof(Tc);
-  constexpr int SR = (kOtherSmem + kThreadWarps * SR0 * kSegStride * 8 <= 48 * 1024 - 256) ? SR0 : 0;
+  constexpr int kOtherSmem = kBoysTableDoubles * 8 + kThreadWarps * 3 * EA * (int)sizeof(Tc) + kThreadWarps * 64;
+  constexpr int SR = (thread_min_blocks(LA + LB + LC + LD) == 1 &&
+                      kOtherSmem + kThreadWarps * SR0 * kSegStride * 8 <= 48 * 1024 - 256)
+                         ? SR0
+                         : 0;
   __shared__ double tab[kBoysTableDoubles];
   __shared__ Tc ebra_all[kThreadWarps][3 * EA];
+  __shared__ double bra_sh[kThreadWarps][8];
   __shared__ double segbuf[kThreadWarps][SR > 0 ? SR * kSegStride : 1];
   for (int i = threadIdx.x; i < kBoysTableDoubles; i += blockDim.x) tab[i] = a.boys[i];
   __syncthreads();
   unsigned long long cnt_q = 0, cnt_p = 0, cnt_s = 0;
   double *sbuf = SR > 0 ? segbuf[threadIdx.x >> 5] : nullptr;
-  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, ebra_all[threadIdx.x >> 5], sbuf, cnt_q,
+  jk_thread_dispatch<LA, LB, LC, LD, Tc, CA, 0, K1>(blockIdx.y, a, tab, ebra_all[threadIdx.x >> 5], sbuf,
+                                                bra_sh[threadIdx.x >> 5], cnt_q,
                                                 cnt_p, cnt_s);
   if (a.counters) {
     const int lane = threadIdx.x & 31;
