@@ -44,8 +44,12 @@ __device__ __forceinline__ void seg_end(int key, int lane, bool &head, int &end)
   end = after ? __ffs(after) - 2 : 31;
 }
 
-// K_ac/K_bc runs with at most kSegMaxValues values per lane are summed
-// before their atomics; from kSegRowsMin values on, through shared memory.
+// K_ac/K_bc blocks of kSegMinValues to kSegMaxValues values per lane sum
+// runs of lanes before their atomics; from kSegRowsMin values on, through
+// shared memory.  Smaller blocks add one atomic per lane: measured on
+// (H2O)32 / cc-pVDZ, per-lane atomics were faster for 2 to 6 values
+// ((ss|ss) 9%, (ps|ss) 5%, (pp|ss) 7%, (ds|ss) 12%).
+constexpr int kSegMinValues = 7;
 constexpr int kSegMaxValues = 18;
 constexpr int kSegRowsMin = 8;
 constexpr int kSegStride = 33;  // doubles per row of a warp's buffer (32 lanes + 1 against bank conflicts)
@@ -155,7 +159,7 @@ __device__ __forceinline__ void jk_digest(const JKArgs &a, const double *g, bool
                                           bool jon, double *sbuf = nullptr) {
   // Segmented reduction of K_ac and K_bc where it is cheap next to the atomics it saves.
   constexpr int NV = (FA + FB) * FC;
-  constexpr bool SEG = NV <= kSegMaxValues;
+  constexpr bool SEG = NV >= kSegMinValues && NV <= kSegMaxValues;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   double w = 0.0;
