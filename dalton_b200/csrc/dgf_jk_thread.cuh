@@ -47,9 +47,10 @@ __device__ __forceinline__ void seg_end(int key, int lane, bool &head, int &end)
 // K_ac/K_bc blocks of kSegMinValues to kSegMaxValues values per lane sum
 // runs of lanes before their atomics; from kSegRowsMin values on, through
 // shared memory.  Smaller blocks add one atomic per lane: measured on
-// (H2O)32 / cc-pVDZ, per-lane atomics were faster for 2 to 6 values
-// ((ss|ss) 9%, (ps|ss) 5%, (pp|ss) 7%, (ds|ss) 12%).
-constexpr int kSegMinValues = 7;
+// (H2O)32 / cc-pVDZ, per-lane atomics were faster for 2 to 10 values
+// ((ss|ss) 9%, (ps|ss) 5%, (pp|ss) 7%, (ds|ss) 12%, (dp|ss) 10%, (dd|ss)
+// 9%) and slower for the 12 of (ps|ps) (15.5 against 13.4 ms).
+constexpr int kSegMinValues = 11;
 constexpr int kSegMaxValues = 18;
 constexpr int kSegRowsMin = 8;
 constexpr int kSegStride = 33;  // doubles per row of a warp's buffer (32 lanes + 1 against bank conflicts)
@@ -658,8 +659,8 @@ __device__ __forceinline__ void jk_thread_dispatch(int chunk, const JKArgs &a, c
 }
 
 // Rows of the shared-memory run buffer a class needs: the largest K_ac/K_bc
-// value count in [kSegRowsMin, kSegMaxValues] over its A chunks, spherical
-// and Cartesian (0: the class reduces its runs with shuffles only).
+// value count in [max(kSegRowsMin, kSegMinValues), kSegMaxValues] over its A
+// chunks, spherical and Cartesian (0: no run buffer).
 template <int LA, int LB, int LC, int CA>
 constexpr int seg_rows_needed() {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC);
@@ -670,7 +671,7 @@ constexpr int seg_rows_needed() {
     const int fa = LA >= 2 ? 2 * LA + 1 : nac;
     const int nv[2] = {(nac + NB) * NC, (fa + FB) * FC};
     for (int v : nv)
-      if (v >= kSegRowsMin && v <= kSegMaxValues && v > best) best = v;
+      if (v >= kSegRowsMin && v >= kSegMinValues && v <= kSegMaxValues && v > best) best = v;
   }
   return best;
 }
